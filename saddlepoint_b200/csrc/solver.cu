@@ -1,0 +1,1138 @@
+// solver.cu — the device-resident solve: GPU scaling passes and transpose,
+// power iteration, PDHG epochs captured as CUDA graphs, and the controller that
+// makes the reference's host-side decisions on the device.
+//
+// Restates crates/saddlepoint-core/src/solver.rs:185-480 (Solver::new, run,
+// estimate_norm, kkt, fixed_point_residual, infeasibility, PidState) and
+// crates/saddlepoint-core/src/scaling.rs:53-103 (ScaledProblem::new).
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "control.cuh"
+#include "internal.cuh"
+#include "solver_kernels.cuh"
+#include "solver_state.h"
+
+namespace sp {
+
+#define GRID_LOOP(i, n) for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// ============================================================ controller
+
+struct CtrlArgs {
+    const double *partP, *partD, *partT, *partP0, *partD0;
+    int nP, nD;  // tiles of A'ᵀ and of A'
+    int E;       // iterations in this epoch
+    sp_check_record *trace;
+    long long trace_cap;
+};
+
+// Sums slot q of a [tiles x NP] partial array in tile order per thread, then a fixed tree.
+template <int NPQ>
+__device__ void sum_slots(const double *part, int tiles, double (&out)[NPQ], double *sh) {
+    double v[NPQ];
+#pragma unroll
+    for (int q = 0; q < NPQ; ++q) v[q] = 0.0;
+    for (int t = threadIdx.x; t < tiles; t += NT)
+#pragma unroll
+        for (int q = 0; q < NPQ; ++q) v[q] += part[t * NPQ + q];
+    block_sum<NPQ>(v, sh);
+#pragma unroll
+    for (int q = 0; q < NPQ; ++q) out[q] = v[q];  // valid in thread 0
+}
+
+// The end of an epoch: the check iteration's decisions (solver.rs:339-419).
+__global__ void __launch_bounds__(NT) k_controller(CtrlArgs a, const DevParams *p, DevState *st) {
+    __shared__ double sh[NP_P * (NT / 32)];
+    if (st->done) return;
+    double P[NP_P], D[NP_D], T[NP_T], P0[1], D0[2];
+    sum_slots<NP_P>(a.partP, a.nP, P, sh);
+    sum_slots<NP_D>(a.partD, a.nD, D, sh);
+    sum_slots<NP_T>(a.partT, a.nP, T, sh);
+    const bool k0_first = st->k == 0 && a.E >= 2;
+    if (k0_first) {
+        sum_slots<1>(a.partP0, a.nP, P0, sh);
+        sum_slots<2>(a.partD0, a.nD, D0, sh);
+    }
+    if (threadIdx.x != 0) return;
+    bool bad = false;
+    if (k0_first) st->anchor_residual = fixed_point_residual(p->eta, st->omega, P0[0], D0[0], D0[1], &bad);
+    const unsigned long long kc = st->k + (unsigned long long)(a.E - 1);  // k of the check iteration
+    const unsigned long long total = st->total + (unsigned long long)a.E;
+    sp_check_record rec;
+    check_decide(st, p, P, D, T, kc, total, &bad, &rec);
+    if (bad) return;
+    if ((long long)st->checks - 1 < a.trace_cap) a.trace[st->checks - 1] = rec;
+    st->trace_len = st->checks;
+}
+// After the check iteration: Halpern step, or the restart's copies (solver.rs:361-362, 411-415).
+__global__ void k_finish(SolverPtrs s, int64_t n, int64_t m) {
+    const DevState *st = s.st;
+    if (st->done) return;
+    const double w = st->w_last, rho = s.prm->reflection;
+    const int rs = st->restart_flag;
+    const bool y32 = s.mixed && !st->fp64;
+    GRID_LOOP(j, n) {
+        if (rs) {
+            const double t = s.xt[j];
+            s.xa[j] = t;
+            s.x[j] = t;
+        } else {
+            s.x[j] = halpern(s.x[j], s.xt[j], s.xa[j], w, rho);
+        }
+    }
+    GRID_LOOP(i, m) {
+        double v;
+        if (rs) {
+            v = s.yt[i];
+            s.ya[i] = v;
+        } else {
+            v = halpern(s.y[i], s.yt[i], s.ya[i], w, rho);
+        }
+        s.y[i] = v;
+        if (y32) s.y32[i] = (float)v;
+    }
+}
+
+// Halpern step of x in the k == 0 iteration that opens an epoch (D did y already).
+__global__ void k_halpern_x0(SolverPtrs s, int64_t n) {
+    const DevState *st = s.st;
+    if (st->done || st->k != 0) return;
+    const double w = 1.0 / 2.0, rho = s.prm->reflection;  // (k + 1) / (k + 2) at k = 0
+    GRID_LOOP(j, n) { s.x[j] = halpern(s.x[j], s.xt[j], s.xa[j], w, rho); }
+}
+
+// ============================================================ power iteration
+
+__global__ void k_power_init(double *v, int64_t n, double *part) {
+    // start = 1 + 0.01 (j mod 7) (solver.rs:221); one block reduces ‖start‖² in order.
+    __shared__ double sh[NT / 32];
+    double s[1] = {0.0};
+    for (int64_t j = threadIdx.x; j < n; j += NT) {
+        const double x = 1.0 + 0.01 * (double)(j % 7);
+        v[j] = x;
+        s[0] += x * x;
+    }
+    block_sum<1>(s, sh);
+    if (threadIdx.x == 0) part[0] = s[0];
+}
+
+__global__ void k_power_start(const double *part, DevState *st) {
+    if (threadIdx.x) return;
+    st->pi_scale = 1.0 / sqrt(part[0]);  // solver.rs:223
+    st->pi_lambda = 0.0;
+    st->pi_done = 0;
+    st->pi_iters = 0;
+    st->error = ERR_NONE;
+}
+
+__global__ void __launch_bounds__(NT) k_power_fin(const double *part, int tiles, unsigned long long max_iters,
+                                                  DevState *st) {
+    __shared__ double sh[NT / 32];
+    if (st->pi_done) return;
+    double s[1];
+    sum_slots<1>(part, tiles, s, sh);
+    if (threadIdx.x) return;
+    const double norm = sqrt(s[0]);  // solver.rs:229-238
+    if (isnan(norm) || norm <= 0.0 || isinf(norm)) {
+        st->error = ERR_NUMERICAL_POWER;
+        st->pi_done = 1;
+        return;
+    }
+    st->pi_scale = 1.0 / norm;
+    const bool done = fabs(norm - st->pi_lambda) <= 1e-6 * norm;
+    st->pi_lambda = norm;
+    st->pi_iters += 1;
+    if (done || (unsigned long long)st->pi_iters >= max_iters) st->pi_done = 1;
+}
+
+// ============================================================ scaling passes (scaling.rs:53-103)
+
+__device__ __forceinline__ double inv_sqrt_d(double v) {  // scaling.rs:139-141
+    return (v > 0.0 && isfinite(v)) ? 1.0 / sqrt(v) : 1.0;
+}
+
+// Per-row geometric-mean factor 1/sqrt(min·max) of |a| (scaling.rs:62-63, min_max :159-178).
+__global__ void k_row_geo(const int *rp, const double *v, int64_t rows, double *f) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < rows; r += nw) {
+        double lo = INFINITY, hi = 0.0;
+        for (int k = rp[r] + lane; k < rp[r + 1]; k += 32) {
+            const double a = fabs(v[k]);
+            lo = fmin(lo, a);
+            hi = fmax(hi, a);
+        }
+        for (int o = 16; o; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            if (hi == 0.0) lo = 0.0;
+            f[r] = inv_sqrt_d(lo * hi);
+        }
+    }
+}
+
+// Per-row Ruiz factor 1/sqrt(max |a|) (scaling.rs:70-72).
+__global__ void k_row_ruiz(const int *rp, const double *v, int64_t rows, double *f) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < rows; r += nw) {
+        double hi = 0.0;
+        for (int k = rp[r] + lane; k < rp[r + 1]; k += 32) hi = fmax(hi, fabs(v[k]));
+        for (int o = 16; o; o >>= 1) hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        if (lane == 0) f[r] = inv_sqrt_d(hi);
+    }
+}
+
+// Per-row Pock-Chambolle factor 1/sqrt(Σ|a|^α), summed in column order from 0.0
+// like abs_stats (scaling.rs:144-155), one thread per row.
+__global__ void k_row_pc(const int *rp, const double *v, int64_t rows, double alpha, double *f) {
+    GRID_LOOP(r, rows) {
+        double s = 0.0;
+        for (int k = rp[r]; k < rp[r + 1]; ++k) {
+            const double a = fabs(v[k]);
+            s = s + (alpha == 1.0 ? a : pow(a, alpha));
+        }
+        f[r] = inv_sqrt_d(s);
+    }
+}
+
+// values[k] *= r[i] * c[j] for every entry (i, j) (CsrMatrix::scale, problem.rs:120-126),
+// applied to A' (rows i) and, in the same pass over its own layout, to A'ᵀ.
+__global__ void k_apply_rows(const int *rp, const int *ci, double *v, int64_t rows, const double *r, const double *c,
+                             int transposed) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < rows; i += nw) {
+        for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
+            const int j = ci[k];
+            // A'ᵀ row i is column i of A': the factor is still r[row] * c[col].
+            const double f = transposed ? r[j] * c[i] : r[i] * c[j];
+            v[k] *= f;
+        }
+    }
+}
+
+__global__ void k_mul_inplace(double *s, const double *f, int64_t n) {
+    GRID_LOOP(i, n) { s[i] *= f[i]; }
+}
+__global__ void k_fill(double *v, double x, int64_t n) {
+    GRID_LOOP(i, n) { v[i] = x; }
+}
+
+// c' = c·C, lc' = lc·R, uc' = uc·R, lv' = lv/C, uv' = uv/C (scaling.rs:83-87).
+__global__ void k_scale_vectors(const double *c, const double *lc, const double *uc, const double *lv, const double *uv,
+                                const double *rs, const double *cs, double *c2, double *lc2, double *uc2, double *lv2,
+                                double *uv2, int64_t m, int64_t n) {
+    GRID_LOOP(j, n) {
+        c2[j] = c[j] * cs[j];
+        lv2[j] = lv[j] / cs[j];
+        uv2[j] = uv[j] / cs[j];
+    }
+    GRID_LOOP(i, m) {
+        lc2[i] = lc[i] * rs[i];
+        uc2[i] = uc[i] * rs[i];
+    }
+}
+
+// The four norms the solve needs, each a sequential sum from -0.0 in index order,
+// as the reference computes them (scaling.rs:186-201): finite_bound_norm and norm2
+// of the scaled bounds and objective, and of the original ones (solver.rs:317-318).
+// One thread per norm: this runs once per solve.
+__global__ void k_seq_norms(const double *lc, const double *uc, int64_t m, const double *c, int64_t n, double *out,
+                            int which) {
+    if (threadIdx.x != 0) return;
+    double s = -0.0;
+    if (which == 0) {
+        for (int64_t i = 0; i < m; ++i) {
+            const double l = isfinite(lc[i]) ? lc[i] : 0.0;
+            const double u = isfinite(uc[i]) ? uc[i] : 0.0;
+            s += (l == u) ? l * l : l * l + u * u;
+        }
+    } else {
+        for (int64_t j = 0; j < n; ++j) s += c[j] * c[j];
+    }
+    out[0] = sqrt(s);
+}
+
+__global__ void k_rescale(double *lc, double *uc, double *lv, double *uv, double *c, const double *norms, int64_t m,
+                          int64_t n, int enabled, double *scales) {
+    const double bs = enabled ? 1.0 / (1.0 + norms[0]) : 1.0;  // scaling.rs:91-92
+    const double os = enabled ? 1.0 / (1.0 + norms[1]) : 1.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scales[0] = bs;
+        scales[1] = os;
+    }
+    if (!enabled) return;
+    GRID_LOOP(i, m) {
+        lc[i] *= bs;
+        uc[i] *= bs;
+    }
+    GRID_LOOP(j, n) {
+        lv[j] *= bs;
+        uv[j] *= bs;
+        c[j] *= os;
+    }
+}
+
+__global__ void k_factors(const double *rs, const double *cs, const double *scales, double *pf, double *df, int64_t m,
+                          int64_t n) {
+    const double bs = scales[0], os = scales[1];
+    GRID_LOOP(i, m) { pf[i] = 1.0 / (rs[i] * bs); }  // scaling.rs:124-126
+    GRID_LOOP(j, n) { df[j] = 1.0 / (cs[j] * os); }  // scaling.rs:129-131
+}
+
+__global__ void k_to_f32(const double *v, float *o, int64_t n) {
+    GRID_LOOP(i, n) { o[i] = (float)v[i]; }
+}
+
+// Transpose helpers: the row of every nonzero, then A'ᵀ from a stable sort by column.
+__global__ void k_row_ids(const int *rp, int64_t rows, int *row_of) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < rows; i += nw)
+        for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) row_of[k] = (int)i;
+}
+__global__ void k_iota(int *v, int64_t n) {
+    GRID_LOOP(i, n) { v[i] = (int)i; }
+}
+// A'ᵀ row pointers from the sorted column keys: rp_t[j] = first position with key >= j.
+__global__ void k_rowptr_from_sorted(const int *keys, int64_t nnz, int64_t ncols, int *rp_t) {
+    GRID_LOOP(j, ncols + 1) {
+        int64_t lo = 0, hi = nnz;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (keys[mid] < j) lo = mid + 1;
+            else hi = mid;
+        }
+        rp_t[j] = (int)lo;
+    }
+}
+__global__ void k_gather_transpose(const int *perm, const int *row_of, const double *v, int *ci_t, double *v_t,
+                                   int64_t nnz) {
+    GRID_LOOP(k, nnz) {
+        const int src = perm[k];
+        ci_t[k] = row_of[src];
+        v_t[k] = v[src];
+    }
+}
+
+// x = x_t C / β, y = y_t R / γ (scaling.rs:113-121).
+__global__ void k_unscale(const double *xt, const double *yt, const double *cs, const double *rs, const double *scales,
+                          double *x, double *y, int64_t n, int64_t m) {
+    const double bs = scales[0], os = scales[1];
+    GRID_LOOP(j, n) { x[j] = xt[j] * cs[j] / bs; }
+    GRID_LOOP(i, m) { y[i] = yt[i] * rs[i] / os; }
+}
+
+}  // namespace sp
+
+// ============================================================ host side
+
+using namespace sp;
+
+namespace {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int grid_of(const sp_ctx *ctx, int64_t n, int per_thread_items = 1) {
+    int64_t b = (n / per_thread_items + NT - 1) / NT;
+    int64_t cap = (int64_t)ctx->sms * 16;
+    return (int)std::max<int64_t>(1, std::min(b, cap));
+}
+
+template <class T>
+int dalloc(T **p, int64_t n) {
+    SP_CUDA_TRY(cudaMalloc(p, sizeof(T) * std::max<int64_t>(n, 1)));
+    return SP_OK;
+}
+
+}  // namespace
+
+namespace sp {
+
+size_t smem_P() { return std::max(tile_smem_bytes<1, double>(), (size_t)(NP_P * (NT / 32) * 8)); }
+size_t smem_D() { return std::max(tile_smem_bytes<4, double>(), (size_t)(NP_D * (NT / 32) * 8)); }
+size_t smem_T() { return tile_smem_bytes<2, double>(); }
+
+// Everything a pass needs, by value.
+SolverPtrs ptrs_of(sp_solver *s) {
+    SolverPtrs p{};
+    p.a_rp = s->A.rp;
+    p.a_ci = s->A.ci;
+    p.a_v = s->A.v;
+    p.a_v32 = s->A.v32;
+    p.a_tiles = s->A.tiles;
+    p.t_rp = s->AT.rp;
+    p.t_ci = s->AT.ci;
+    p.t_v = s->AT.v;
+    p.t_v32 = s->AT.v32;
+    p.t_tiles = s->AT.tiles;
+    p.c = s->c;
+    p.lc = s->lc;
+    p.uc = s->uc;
+    p.lv = s->lv;
+    p.uv = s->uv;
+    p.pf = s->pf;
+    p.df = s->df;
+    p.x = s->x;
+    p.y = s->y;
+    p.xt = s->xt;
+    p.yt = s->yt;
+    p.xbar = s->xbar;
+    p.xa = s->xa;
+    p.ya = s->ya;
+    p.aty = s->aty;
+    p.xbar32 = s->xbar32;
+    p.y32 = s->y32;
+    p.partP = s->partP;
+    p.partD = s->partD;
+    p.partT = s->partT;
+    p.partP0 = s->partP0;
+    p.partD0 = s->partD0;
+    p.prm = s->d_prm;
+    p.st = s->d_st;
+    p.mixed = s->mixed;
+    return p;
+}
+
+template <bool LO, int MODE>
+PrimalPass<LO, MODE> mkP(const SolverPtrs &p, int i, int role) {
+    PrimalPass<LO, MODE> o{};
+    o.rp = p.t_rp;
+    o.ci = p.t_ci;
+    if constexpr (LO) o.vals = p.t_v32;
+    else o.vals = p.t_v;
+    o.tiles = p.t_tiles;
+    o.s = p;
+    o.i = i;
+    o.role = role;
+    return o;
+}
+template <bool LO, int MODE>
+DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
+    DualPass<LO, MODE> o{};
+    o.rp = p.a_rp;
+    o.ci = p.a_ci;
+    if constexpr (LO && MODE == 0) o.vals = p.a_v32;
+    else o.vals = p.a_v;
+    o.tiles = p.a_tiles;
+    o.s = p;
+    o.i = i;
+    o.role = role;
+    return o;
+}
+
+// Launches the primal pass of iteration i with the given role.
+void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
+    const SolverPtrs p = ptrs_of(s);
+    const int g = s->AT.ntiles;
+    if (g == 0) return;
+    const size_t sm = smem_P();
+    if (s->mixed) {
+        if (role == ROLE_MID)
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
+        else if (role == ROLE_FIRST)
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<true, 1>(p, i, role), mkP<false, 0>(p, i, role),
+                                           mkP<false, 1>(p, i, role));
+        else
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 2>(p, i, role), mkP<false, 2>(p, i, role));
+    } else {
+        if (role == ROLE_MID) k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
+        else if (role == ROLE_FIRST)
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role), mkP<false, 1>(p, i, role));
+        else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 2>(p, i, role));
+    }
+}
+
+void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
+    const SolverPtrs p = ptrs_of(s);
+    const int g = s->A.ntiles;
+    if (g == 0) return;
+    const size_t sm = smem_D();
+    if (s->mixed) {
+        if (role == ROLE_MID)
+            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
+        else if (role == ROLE_FIRST)
+            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<true, 1>(p, i, role),
+                                                                     mkD<false, 0>(p, i, role), mkD<false, 1>(p, i, role));
+        else
+            k_tiles_any<<<g, NT, sm, st>>>(mkD<true, 2>(p, i, role), mkD<false, 2>(p, i, role));
+    } else {
+        if (role == ROLE_MID)
+            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<false, 0>(p, i, role));
+        else if (role == ROLE_FIRST)
+            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<false, 0>(p, i, role), mkD<false, 1>(p, i, role));
+        else k_tiles_any<<<g, NT, sm, st>>>(mkD<false, 2>(p, i, role));
+    }
+}
+
+void launch_T(sp_solver *s, int i, cudaStream_t st) {
+    const SolverPtrs p = ptrs_of(s);
+    if (s->AT.ntiles == 0) return;
+    CheckPassT o{};
+    o.rp = p.t_rp;
+    o.ci = p.t_ci;
+    o.vals = p.t_v;
+    o.tiles = p.t_tiles;
+    o.s = p;
+    o.i = i;
+    k_tiles_any<<<s->AT.ntiles, NT, smem_T(), st>>>(o);
+}
+
+// One epoch of E iterations (the last is the check) on stream `st`. With timing
+// on, CUDA events bracket the P and D launches of sampled MID iterations.
+void enqueue_epoch(sp_solver *s, int E, cudaStream_t st, bool timed) {
+    const SolverPtrs p = ptrs_of(s);
+    const int gn = grid_of(s->ctx, std::max(s->n, s->m));
+    for (int i = 0; i < E; ++i) {
+        const bool last = i == E - 1;
+        const int role = last ? ROLE_CHECK : (i == 0 ? ROLE_FIRST : ROLE_MID);
+        const bool sample = timed && role == ROLE_MID && s->timing_every > 0 && (s->timing_counter++ % s->timing_every == 0);
+        cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+        if (sample) {
+            e0 = s->event();
+            e1 = s->event();
+            e2 = s->event();
+            cudaEventRecord(e0, st);
+        }
+        launch_P(s, i, role, st);
+        if (sample) cudaEventRecord(e1, st);
+        launch_D(s, i, role, st);
+        if (sample) {
+            cudaEventRecord(e2, st);
+            s->samples.push_back({e0, e1, e2});
+        }
+        if (role == ROLE_FIRST) k_halpern_x0<<<gn, NT, 0, st>>>(p, s->n);
+        if (last) {
+            launch_T(s, i, st);
+            CtrlArgs a{s->partP, s->partD, s->partT, s->partP0, s->partD0, s->AT.ntiles, s->A.ntiles, E, s->d_trace,
+                       (long long)s->trace_cap};
+            k_controller<<<1, NT, 0, st>>>(a, s->d_prm, s->d_st);
+            k_finish<<<gn, NT, 0, st>>>(p, s->n, s->m);
+        }
+    }
+}
+
+int set_smem_limits() {
+    static bool done = false;
+    if (done) return SP_OK;
+    // Opt in to more than 48 KB of dynamic shared memory for the 4-product check pass.
+    auto set = [](const void *f, size_t bytes) {
+        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    using DL0 = DualPass<true, 2>;
+    using DH0 = DualPass<false, 2>;
+    SP_CUDA_TRY(set((const void *)k_tiles_any<DL0, DH0>, smem_D()));
+    SP_CUDA_TRY(set((const void *)k_tiles_any<DH0>, smem_D()));
+    done = true;
+    return SP_OK;
+}
+
+int build_graph(sp_solver *s, int E, cudaGraphExec_t *out) {
+    cudaStream_t st = s->ctx->stream;
+    cudaGraph_t g;
+    SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_epoch(s, E, st, false);
+    SP_CUDA_TRY(cudaStreamEndCapture(st, &g));
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(SP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return SP_OK;
+}
+
+}  // namespace sp
+
+// ------------------------------------------------------------------ creation
+
+namespace sp {
+
+void solver_release(sp_solver *s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
+    free_csr(&s->A);
+    free_csr(&s->AT);
+    void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
+                    s->aty, s->xbar32, s->y32, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
+                    s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,
+                    s->out_x, s->out_y};
+    for (void *b : bufs) cudaFree(b);
+    cudaFreeHost(s->h_st);
+    delete s;
+}
+
+// Scaling passes on the device (ScaledProblem::new, scaling.rs:53-103). A' and
+// A'ᵀ are kept in step: each pass multiplies both by the same r_i * c_j products.
+int scale_on_device(sp_solver *s, const sp_lp *lp) {
+    sp_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int64_t m = s->m, n = s->n, nnz = s->nnz;
+    const sp_solver_params &P = s->prm;
+    double *r, *c, *ones_m, *ones_n;
+    int rc;
+    if ((rc = dalloc(&r, m)) || (rc = dalloc(&c, n)) || (rc = dalloc(&ones_m, m)) || (rc = dalloc(&ones_n, n))) return rc;
+    const int gm = grid_of(ctx, m), gn = grid_of(ctx, n);
+    const int wm = grid_of(ctx, m * 32), wn = grid_of(ctx, n * 32);
+    k_fill<<<gm, NT, 0, st>>>(ones_m, 1.0, m);
+    k_fill<<<gn, NT, 0, st>>>(ones_n, 1.0, n);
+    k_fill<<<gm, NT, 0, st>>>(s->row_scale, 1.0, m);
+    k_fill<<<gn, NT, 0, st>>>(s->col_scale, 1.0, n);
+    auto apply = [&](const double *rr, const double *cc) {  // apply (scaling.rs:180-184)
+        if (nnz) {
+            k_apply_rows<<<wm, NT, 0, st>>>(s->A.rp, s->A.ci, s->A.v, m, rr, cc, 0);
+            k_apply_rows<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.ci, s->AT.v, n, rr, cc, 1);
+        }
+        k_mul_inplace<<<gm, NT, 0, st>>>(s->row_scale, rr, m);
+        k_mul_inplace<<<gn, NT, 0, st>>>(s->col_scale, cc, n);
+    };
+    for (uint64_t pass = 0; pass < P.geometric_mean_passes; ++pass) {
+        k_row_geo<<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, r);
+        apply(r, ones_n);
+        k_row_geo<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, c);
+        apply(ones_m, c);
+    }
+    for (uint64_t it = 0; it < P.ruiz_iterations; ++it) {
+        k_row_ruiz<<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, r);
+        k_row_ruiz<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, c);
+        apply(r, c);
+    }
+    if (P.pock_chambolle_enabled) {
+        k_row_pc<<<gm, NT, 0, st>>>(s->A.rp, s->A.v, m, P.pock_chambolle_alpha, r);
+        k_row_pc<<<gn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, 2.0 - P.pock_chambolle_alpha, c);
+        apply(r, c);
+    }
+    // Original bounds and objective come in through the output slots of the scaled ones.
+    double *oc, *olc, *ouc, *olv, *ouv;
+    if ((rc = upload_vec(ctx, &oc, lp->c, n)) || (rc = upload_vec(ctx, &olc, lp->lc, m)) ||
+        (rc = upload_vec(ctx, &ouc, lp->uc, m)) || (rc = upload_vec(ctx, &olv, lp->lv, n)) ||
+        (rc = upload_vec(ctx, &ouv, lp->uv, n)))
+        return rc;
+    // norms of the original problem (solver.rs:317-318)
+    k_seq_norms<<<1, 32, 0, st>>>(olc, ouc, m, oc, n, s->norms + 2, 0);
+    k_seq_norms<<<1, 32, 0, st>>>(olc, ouc, m, oc, n, s->norms + 3, 1);
+    k_scale_vectors<<<std::max(gm, gn), NT, 0, st>>>(oc, olc, ouc, olv, ouv, s->row_scale, s->col_scale, s->c, s->lc,
+                                                     s->uc, s->lv, s->uv, m, n);
+    k_seq_norms<<<1, 32, 0, st>>>(s->lc, s->uc, m, s->c, n, s->norms + 0, 0);
+    k_seq_norms<<<1, 32, 0, st>>>(s->lc, s->uc, m, s->c, n, s->norms + 1, 1);
+    k_rescale<<<std::max(gm, gn), NT, 0, st>>>(s->lc, s->uc, s->lv, s->uv, s->c, s->norms, m, n,
+                                               P.bound_objective_rescaling, s->scales);
+    k_factors<<<std::max(gm, gn), NT, 0, st>>>(s->row_scale, s->col_scale, s->scales, s->pf, s->df, m, n);
+    SP_CUDA_TRY(cudaGetLastError());
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    for (double *b : {r, c, ones_m, ones_n, oc, olc, ouc, olv, ouv}) cudaFree(b);
+    return SP_OK;
+}
+
+// A'ᵀ on the device: a stable radix sort of the column indices (cub) gives, per
+// column, its entries in increasing row order: CsrMatrix::transpose's order
+// (problem.rs:88-109), bit for bit.
+int transpose_on_device(sp_solver *s) {
+    sp_ctx *ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const int64_t m = s->m, n = s->n, nnz = s->nnz;
+    DevCsr &T = s->AT;
+    T.nrows = n;
+    T.ncols = m;
+    T.nnz = nnz;
+    int rc;
+    if ((rc = dalloc(&T.rp, n + 1)) || (rc = dalloc(&T.ci, nnz)) || (rc = dalloc(&T.v, nnz))) return rc;
+    int *row_of, *keys_out, *perm_in, *perm_out;
+    if ((rc = dalloc(&row_of, nnz)) || (rc = dalloc(&keys_out, nnz)) || (rc = dalloc(&perm_in, nnz)) ||
+        (rc = dalloc(&perm_out, nnz)))
+        return rc;
+    k_row_ids<<<grid_of(ctx, m * 32), NT, 0, st>>>(s->A.rp, m, row_of);
+    k_iota<<<grid_of(ctx, nnz), NT, 0, st>>>(perm_in, nnz);
+    int bits = 1;
+    while ((int64_t(1) << bits) < n) ++bits;
+    size_t temp = 0;
+    SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp, s->A.ci, keys_out, perm_in, perm_out, (int)nnz, 0, bits,
+                                                st));
+    void *tmp = nullptr;
+    SP_CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(temp, 1)));
+    SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, s->A.ci, keys_out, perm_in, perm_out, (int)nnz, 0, bits, st));
+    k_rowptr_from_sorted<<<grid_of(ctx, n + 1), NT, 0, st>>>(keys_out, nnz, n, T.rp);
+    k_gather_transpose<<<grid_of(ctx, nnz), NT, 0, st>>>(perm_out, row_of, s->A.v, T.ci, T.v, nnz);
+    SP_CUDA_TRY(cudaGetLastError());
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    for (void *b : {(void *)row_of, (void *)keys_out, (void *)perm_in, (void *)perm_out, tmp}) cudaFree(b);
+    // tile plan of A'ᵀ from its row pointers
+    std::vector<int> rp32(n + 1);
+    SP_CUDA_TRY(cudaMemcpy(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    std::vector<int64_t> rp64(rp32.begin(), rp32.end());
+    std::vector<int2> tiles = build_tiles(rp64.data(), n);
+    T.ntiles = (int)tiles.size();
+    SP_CUDA_TRY(cudaMalloc(&T.tiles, sizeof(int2) * std::max<size_t>(tiles.size(), 1)));
+    if (!tiles.empty())
+        SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+    return SP_OK;
+}
+
+int validate_lp(const sp_lp *lp) {  // LpProblem::validate (problem.rs:166-194)
+    const int64_t m = lp->a.nrows, n = lp->a.ncols;
+    for (int64_t j = 0; j < n; ++j) {
+        if (std::isnan(lp->lv[j]) || std::isnan(lp->uv[j])) return fail(SP_ERR_PROBLEM, "variable bound is NaN");
+        if (lp->lv[j] > lp->uv[j]) return fail(SP_ERR_PROBLEM, "variable has lower bound above upper bound");
+        if (std::isnan(lp->c[j])) return fail(SP_ERR_PROBLEM, "coefficient is NaN");
+    }
+    for (int64_t i = 0; i < m; ++i) {
+        if (std::isnan(lp->lc[i]) || std::isnan(lp->uc[i])) return fail(SP_ERR_PROBLEM, "constraint bound is NaN");
+        if (lp->lc[i] > lp->uc[i]) return fail(SP_ERR_PROBLEM, "constraint has lower bound above upper bound");
+    }
+    for (int64_t k = 0; k < lp->a.nnz; ++k)
+        if (std::isnan(lp->a.values[k])) return fail(SP_ERR_PROBLEM, "coefficient is NaN");
+    return SP_OK;
+}
+
+int power_iteration(sp_solver *s) {  // Solver::estimate_norm (solver.rs:215-242)
+    cudaStream_t st = s->ctx->stream;
+    if (s->n == 0 || s->nnz == 0) {
+        s->norm_est = 1.0;
+        return SP_OK;
+    }
+    k_power_init<<<1, NT, 0, st>>>(s->pv, s->n, s->ppart);
+    k_power_start<<<1, 32, 0, st>>>(s->ppart, s->d_st);
+    const uint64_t maxit = s->prm.power_iterations;
+    PowerA a{s->A.rp, s->A.ci, s->A.v, s->A.tiles, s->pv, s->ptmp, s->d_st, 0.0};
+    PowerT t{s->AT.rp, s->AT.ci, s->AT.v, s->AT.tiles, s->ptmp, s->pv, s->ppart, s->d_st};
+    const uint64_t chunk = 8;
+    DevState h{};  // with no iterations, λ stays 0 as in the reference
+    for (uint64_t done_it = 0; done_it < maxit;) {
+        const uint64_t c = std::min(chunk, maxit - done_it);
+        for (uint64_t q = 0; q < c; ++q) {
+            k_tiles<<<s->A.ntiles, NT, tile_smem_bytes<1, double>(), st>>>(a);
+            k_tiles<<<s->AT.ntiles, NT, tile_smem_bytes<1, double>(), st>>>(t);
+            k_power_fin<<<1, NT, 0, st>>>(s->ppart, s->AT.ntiles, maxit, s->d_st);
+        }
+        done_it += c;
+        SP_CUDA_TRY(cudaMemcpyAsync(&h, s->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+        SP_CUDA_TRY(cudaStreamSynchronize(st));
+        if (h.pi_done) break;
+    }
+    if (h.error == ERR_NUMERICAL_POWER) return fail(SP_ERR_NUMERICAL, "numerical breakdown: power iteration collapsed");
+    s->norm_est = sqrt(h.pi_lambda) * 1.01;  // solver.rs:241
+    s->pi_iters = h.pi_iters;
+    return SP_OK;
+}
+
+}  // namespace sp
+
+extern "C" void sp_solver_params_default(sp_solver_params *p) {
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    p->tolerance = 1e-6;  // solver.rs:70-93
+    p->infeasibility_tolerance = 1e-8;
+    p->max_iterations = 1000000;
+    p->time_limit_s = 0.0;
+    p->check_every = 64;
+    p->step_size_factor = 0.998;
+    p->reflection = 1.0;
+    p->restart_sufficient = 0.2;
+    p->restart_necessary = 0.5;
+    p->restart_artificial = 0.36;
+    p->pid_kp = 0.99;
+    p->pid_ki = 0.01;
+    p->pid_kd = 0.0;
+    p->pid_discount = 0.3;
+    p->power_iterations = 200;
+    p->geometric_mean_passes = 12;  // scaling.rs:25-34
+    p->ruiz_iterations = 10;
+    p->pock_chambolle_enabled = 1;
+    p->pock_chambolle_alpha = 1.0;
+    p->bound_objective_rescaling = 1;
+    p->log_every_checks = 0;
+    p->termination = SP_TERMINATION_PROJECTED;
+    p->precision = SP_PRECISION_FP64;
+    p->mixed_switch_tolerance = 1e-5;
+}
+
+extern "C" int sp_solver_reset(sp_solver *s) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const int64_t m = s->m, n = s->n;
+    for (double *v : {s->x, s->xt, s->xbar, s->xa, s->aty}) SP_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(double) * n, st));
+    for (double *v : {s->y, s->yt, s->ya}) SP_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(double) * m, st));
+    if (s->mixed) {
+        SP_CUDA_TRY(cudaMemsetAsync(s->xbar32, 0, sizeof(float) * n, st));
+        SP_CUDA_TRY(cudaMemsetAsync(s->y32, 0, sizeof(float) * m, st));
+    }
+    DevState h{};
+    h.total = 0;
+    h.k = 0;
+    // Initial primal weight (solver.rs:322).
+    h.omega = s->prm.bound_objective_rescaling ? 1.0 : (1.0 + s->c_norm) / (1.0 + s->b_norm);
+    h.status = -1;
+    h.fp64 = s->mixed ? 0 : 1;
+    h.anchor_residual = INFINITY;
+    h.prev_residual = INFINITY;
+    h.pid_best_weight = h.omega;  // PidState::new (solver.rs:453-455)
+    h.pid_best_balance = INFINITY;
+    h.pi_done = 1;
+    *s->h_st = h;
+    SP_CUDA_TRY(cudaMemcpyAsync(s->d_st, s->h_st, sizeof(DevState), cudaMemcpyHostToDevice, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    s->launched = 0;
+    s->time_limited = false;
+    return SP_OK;
+}
+
+extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *params, sp_solver **out) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!lp || !out || !lp->c || !lp->lc || !lp->uc || !lp->lv || !lp->uv)
+        return fail(SP_ERR_INVALID, "sp_solver_create: null argument");
+    if ((rc = validate_lp(lp))) return rc;
+    double t0 = now_s();
+    auto *s = new sp_solver();
+    s->ctx = ctx;
+    sp_solver_params_default(&s->prm);
+    if (params) s->prm = *params;
+    s->mixed = s->prm.precision == SP_PRECISION_MIXED;
+    s->m = lp->a.nrows;
+    s->n = lp->a.ncols;
+    s->nnz = lp->a.nnz;
+    s->c0 = lp->c0;
+    s->maximize = lp->maximize;
+    if (s->prm.check_every == 0) s->prm.check_every = 1ull << 62;  // never a multiple: only the iteration limit checks
+    const int64_t m = s->m, n = s->n;
+    const int64_t nP = 0;
+    (void)nP;
+    auto cleanup = [&](int code) {
+        solver_release(s);
+        return code;
+    };
+    if ((rc = upload_csr(ctx, &lp->a, &s->A, false))) return cleanup(rc);
+    if ((rc = transpose_on_device(s))) return cleanup(rc);
+    if ((rc = dalloc(&s->c, n)) || (rc = dalloc(&s->lc, m)) || (rc = dalloc(&s->uc, m)) || (rc = dalloc(&s->lv, n)) ||
+        (rc = dalloc(&s->uv, n)) || (rc = dalloc(&s->pf, m)) || (rc = dalloc(&s->df, n)) ||
+        (rc = dalloc(&s->row_scale, m)) || (rc = dalloc(&s->col_scale, n)) || (rc = dalloc(&s->scales, 2)) ||
+        (rc = dalloc(&s->norms, 4)))
+        return cleanup(rc);
+    if ((rc = scale_on_device(s, lp))) return cleanup(rc);
+    double hn[4], hs[2];
+    SP_CUDA_TRY(cudaMemcpy(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost));
+    SP_CUDA_TRY(cudaMemcpy(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost));
+    s->b_norm = hn[2];
+    s->c_norm = hn[3];
+    s->bound_scale = hs[0];
+    s->obj_scale = hs[1];
+    if (s->mixed) {
+        if ((rc = dalloc(&s->A.v32, s->nnz)) || (rc = dalloc(&s->AT.v32, s->nnz))) return cleanup(rc);
+        k_to_f32<<<grid_of(ctx, s->nnz), NT, 0, ctx->stream>>>(s->A.v, s->A.v32, s->nnz);
+        k_to_f32<<<grid_of(ctx, s->nnz), NT, 0, ctx->stream>>>(s->AT.v, s->AT.v32, s->nnz);
+    }
+    if ((rc = dalloc(&s->x, n)) || (rc = dalloc(&s->y, m)) || (rc = dalloc(&s->xt, n)) || (rc = dalloc(&s->yt, m)) ||
+        (rc = dalloc(&s->xbar, n)) || (rc = dalloc(&s->xa, n)) || (rc = dalloc(&s->ya, m)) ||
+        (rc = dalloc(&s->aty, n)) || (rc = dalloc(&s->xbar32, n)) || (rc = dalloc(&s->y32, m)) ||
+        (rc = dalloc(&s->partP, (int64_t)s->AT.ntiles * NP_P)) || (rc = dalloc(&s->partT, (int64_t)s->AT.ntiles * NP_T)) ||
+        (rc = dalloc(&s->partP0, (int64_t)s->AT.ntiles * NP_P0)) ||
+        (rc = dalloc(&s->partD, (int64_t)s->A.ntiles * NP_D)) || (rc = dalloc(&s->partD0, (int64_t)s->A.ntiles * NP_D0)) ||
+        (rc = dalloc(&s->pv, n)) || (rc = dalloc(&s->ptmp, m)) ||
+        (rc = dalloc(&s->ppart, std::max<int64_t>(s->AT.ntiles, 1))) || (rc = dalloc(&s->d_st, 1)) ||
+        (rc = dalloc(&s->d_prm, 1)))
+        return cleanup(rc);
+    s->trace_cap = (int64_t)std::min<uint64_t>(s->prm.max_iterations / std::max<uint64_t>(s->prm.check_every, 1) + 2,
+                                               1 << 20);
+    if ((rc = dalloc(&s->d_trace, s->trace_cap))) return cleanup(rc);
+    SP_CUDA_TRY(cudaMallocHost(&s->h_st, sizeof(DevState) * (SolverLookahead + 2)));
+    if ((rc = set_smem_limits())) return cleanup(rc);
+    // ‖A'‖₂ and η (solver.rs:316)
+    if ((rc = sp_solver_reset(s))) return cleanup(rc);
+    if ((rc = power_iteration(s))) return cleanup(rc);
+    DevParams dp{};
+    const sp_solver_params &P = s->prm;
+    dp.tolerance = P.tolerance;
+    dp.infeasibility_tolerance = P.infeasibility_tolerance;
+    dp.max_iterations = P.max_iterations;
+    dp.check_every = P.check_every;
+    dp.reflection = P.reflection;
+    dp.restart_sufficient = P.restart_sufficient;
+    dp.restart_necessary = P.restart_necessary;
+    dp.restart_artificial = P.restart_artificial;
+    dp.pid_kp = P.pid_kp;
+    dp.pid_ki = P.pid_ki;
+    dp.pid_kd = P.pid_kd;
+    dp.pid_discount = P.pid_discount;
+    dp.termination = P.termination;
+    dp.mixed = s->mixed;
+    dp.mixed_switch_tolerance = P.mixed_switch_tolerance;
+    dp.b_norm = s->b_norm;
+    dp.c_norm = s->c_norm;
+    dp.c0 = s->c0;
+    dp.obj_factor = 1.0 / (s->bound_scale * s->obj_scale);  // scaling.rs:134-136
+    dp.eta = P.step_size_factor / s->norm_est;
+    dp.bound_objective_rescaling = P.bound_objective_rescaling;
+    SP_CUDA_TRY(cudaMemcpy(s->d_prm, &dp, sizeof dp, cudaMemcpyHostToDevice));
+    if ((rc = sp_solver_reset(s))) return cleanup(rc);
+    s->setup_s = now_s() - t0;
+    *out = s;
+    return SP_OK;
+}
+
+namespace sp {
+
+int epoch_graph(sp_solver *s, int E, cudaGraphExec_t *g) {
+    auto it = s->graphs.find(E);
+    if (it != s->graphs.end()) {
+        *g = it->second;
+        return SP_OK;
+    }
+    int rc = build_graph(s, E, g);
+    if (rc) return rc;
+    s->graphs[E] = *g;
+    return SP_OK;
+}
+
+// Enqueues one epoch (graph, or direct launches when timing samples are due).
+int launch_epoch(sp_solver *s, int E) {
+    cudaStream_t st = s->ctx->stream;
+    if (s->timing_every > 0) {
+        enqueue_epoch(s, E, st, true);
+    } else {
+        cudaGraphExec_t g;
+        int rc = epoch_graph(s, E, &g);
+        if (rc) return rc;
+        SP_CUDA_TRY(cudaGraphLaunch(g, st));
+    }
+    SP_CUDA_TRY(cudaGetLastError());
+    s->launched += (uint64_t)E;
+    return SP_OK;
+}
+
+void fill_info(sp_solver *s, const DevState &h, sp_solution_info *info) {
+    if (!info) return;
+    const double sign = s->maximize ? -1.0 : 1.0;
+    info->status = h.done ? h.status : (s->time_limited ? SP_STATUS_TIME_LIMIT : -1);
+    info->objective = sign * h.primal_obj;
+    info->dual_objective = sign * h.dual_obj;
+    info->primal_residual = h.primal_res;
+    info->dual_residual = h.dual_res;
+    info->gap = fabs(h.primal_obj - h.dual_obj);
+    info->iterations = h.total;
+    info->restarts = h.restarts;
+    info->solve_time_s = s->solve_s;
+    info->setup_time_s = s->setup_s;
+    info->norm_estimate = s->norm_est;
+    info->fp64_from_iteration = s->mixed ? h.fp64_from : 0;
+}
+
+}  // namespace sp
+
+extern "C" int sp_solver_run_epochs(sp_solver *s, uint64_t epochs) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    for (uint64_t e = 0; e < epochs; ++e) {
+        const uint64_t E = std::min<uint64_t>(s->prm.check_every, s->prm.max_iterations - std::min(s->launched, s->prm.max_iterations));
+        if (E == 0) break;
+        if ((rc = launch_epoch(s, (int)E))) return rc;
+    }
+    return SP_OK;
+}
+
+extern "C" int sp_solver_sync(sp_solver *s) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    SP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    return SP_OK;
+}
+
+extern "C" int sp_solver_solve(sp_solver *s, sp_solution_info *info) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const double t0 = now_s();
+    const double limit = s->prm.time_limit_s;
+    // Epochs are queued SolverLookahead ahead of the state the host has seen;
+    // each queued epoch is followed by a copy of the state into its own slot.
+    std::vector<cudaEvent_t> ev(SolverLookahead + 1);
+    for (auto &e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    uint64_t queued = 0, seen = 0;
+    bool stop = false;
+    DevState last{};
+    uint64_t logged_checks = 0;
+    while (!stop) {
+        while (!stop && queued - seen < (uint64_t)SolverLookahead + 1) {
+            const uint64_t E = std::min<uint64_t>(s->prm.check_every,
+                                                  s->prm.max_iterations - std::min(s->launched, s->prm.max_iterations));
+            if (E == 0) {
+                stop = queued == seen;
+                break;
+            }
+            if ((rc = launch_epoch(s, (int)E))) return rc;
+            const int slot = (int)(queued % ev.size());
+            SP_CUDA_TRY(cudaMemcpyAsync(&s->h_st[slot], s->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+            SP_CUDA_TRY(cudaEventRecord(ev[slot], st));
+            ++queued;
+        }
+        if (seen == queued) break;
+        const int slot = (int)(seen % ev.size());
+        SP_CUDA_TRY(cudaEventSynchronize(ev[slot]));
+        last = s->h_st[slot];
+        ++seen;
+        if (s->prm.log_every_checks > 0 && last.checks > logged_checks && last.checks % s->prm.log_every_checks == 0) {
+            logged_checks = last.checks;
+            fprintf(stderr, "%9llu %14.6e %14.6e %9.2e %9.2e %9.2e %9.2e %5llu %8.2fs %7llu %9.2e\n",
+                    (unsigned long long)last.total, last.primal_obj, last.dual_obj, last.primal_res, last.dual_res,
+                    fabs(last.primal_obj - last.dual_obj), last.omega, (unsigned long long)last.restarts,
+                    now_s() - t0, (unsigned long long)last.k, last.last_residual / last.anchor_residual);
+        }
+        if (last.done) stop = true;
+        if (!stop && limit > 0 && now_s() - t0 >= limit) {  // solver.rs:392-394, observed per epoch
+            s->time_limited = true;
+            stop = true;
+        }
+    }
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    for (auto &e : ev) cudaEventDestroy(e);
+    SP_CUDA_TRY(cudaMemcpy(s->h_st, s->d_st, sizeof(DevState), cudaMemcpyDeviceToHost));
+    last = s->h_st[0];
+    s->solve_s = now_s() - t0;
+    if (last.error == ERR_NUMERICAL_ITERATES) return fail(SP_ERR_NUMERICAL, "numerical breakdown: iterates are not finite");
+    if (!last.done && !s->time_limited) s->time_limited = true;  // only reachable with an exhausted limit
+    fill_info(s, last, info);
+    return SP_OK;
+}
+
+extern "C" int sp_solver_info(sp_solver *s, sp_solution_info *info) {
+    if (!s || !info) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    SP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    DevState h;
+    SP_CUDA_TRY(cudaMemcpy(&h, s->d_st, sizeof h, cudaMemcpyDeviceToHost));
+    fill_info(s, h, info);
+    return SP_OK;
+}
+
+extern "C" int sp_solver_download(sp_solver *s, double *x, double *y) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    cudaStream_t st = s->ctx->stream;
+    if (!s->out_x) {
+        if ((rc = dalloc(&s->out_x, s->n)) || (rc = dalloc(&s->out_y, s->m))) return rc;
+    }
+    k_unscale<<<grid_of(s->ctx, std::max(s->n, s->m)), NT, 0, st>>>(s->xt, s->yt, s->col_scale, s->row_scale, s->scales,
+                                                                    s->out_x, s->out_y, s->n, s->m);
+    if (x && s->n) SP_CUDA_TRY(cudaMemcpyAsync(x, s->out_x, sizeof(double) * s->n, cudaMemcpyDeviceToHost, st));
+    if (y && s->m) SP_CUDA_TRY(cudaMemcpyAsync(y, s->out_y, sizeof(double) * s->m, cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
+extern "C" int sp_solver_trace(sp_solver *s, sp_check_record *out, int64_t cap, int64_t *len) {
+    if (!s || !len) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    SP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    DevState h;
+    SP_CUDA_TRY(cudaMemcpy(&h, s->d_st, sizeof h, cudaMemcpyDeviceToHost));
+    const int64_t avail = std::min<int64_t>((int64_t)h.trace_len, s->trace_cap);
+    *len = avail;
+    const int64_t k = std::min(avail, cap);
+    if (k > 0 && out) SP_CUDA_TRY(cudaMemcpy(out, s->d_trace, sizeof(sp_check_record) * k, cudaMemcpyDeviceToHost));
+    return SP_OK;
+}
+
+extern "C" int sp_solver_set_timing(sp_solver *s, int every) {
+    if (!s) return SP_ERR_INVALID;
+    s->timing_every = every > 0 ? every : 0;
+    s->timing_counter = 0;
+    s->samples.clear();
+    s->event_next = 0;
+    return SP_OK;
+}
+
+extern "C" int sp_solver_kernel_timing(sp_solver *s, int id, int64_t *launches, double *total_ms,
+                                       double *bytes_per_launch) {
+    if (!s || id < 0 || id > 1) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    SP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    double tot = 0.0;
+    int64_t cnt = 0;
+    for (auto &smp : s->samples) {
+        float ms = 0.f;
+        cudaEvent_t a = id == 0 ? smp.e0 : smp.e1, b = id == 0 ? smp.e1 : smp.e2;
+        if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) {
+            tot += ms;
+            ++cnt;
+        }
+    }
+    if (launches) *launches = cnt;
+    if (total_ms) *total_ms = tot;
+    if (bytes_per_launch) *bytes_per_launch = s->pass_bytes(id);
+    return SP_OK;
+}
+
+extern "C" double sp_solver_bytes_per_iteration(sp_solver *s) { return s ? s->pass_bytes(0) + s->pass_bytes(1) : 0.0; }
+
+extern "C" void sp_solver_free(sp_solver *s) { solver_release(s); }
+
+// The whole solve in one call (Part 2).
+extern "C" int sp_solve(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *params, double *x, double *y,
+                        sp_solution_info *info) {
+    sp_solver *s = nullptr;
+    int rc = sp_solver_create(ctx, lp, params, &s);
+    if (rc) return rc;
+    rc = sp_solver_solve(s, info);
+    if (!rc) rc = sp_solver_download(s, x, y);
+    if (!rc && info) {
+        info->setup_time_s = s->setup_s;
+        info->solve_time_s = s->solve_s;
+    }
+    sp_solver_free(s);
+    return rc;
+}
+
+extern "C" int sp_solver_scaled(sp_solver *s, int64_t *a_row_ptr, int32_t *a_col_idx, double *a_values,
+                                int64_t *at_row_ptr, int32_t *at_col_idx, double *at_values, double *c, double *lc,
+                                double *uc, double *lv, double *uv, double *row_scale, double *col_scale,
+                                double *bound_scale, double *obj_scale) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    SP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    const int64_t m = s->m, n = s->n, nnz = s->nnz;
+    auto rowptr = [&](const int *d, int64_t rows, int64_t *out) -> int {
+        if (!out) return SP_OK;
+        std::vector<int> tmp(rows + 1);
+        SP_CUDA_TRY(cudaMemcpy(tmp.data(), d, sizeof(int) * (rows + 1), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i <= rows; ++i) out[i] = tmp[i];
+        return SP_OK;
+    };
+    auto copy = [&](void *dst, const void *src, size_t bytes) -> int {
+        if (dst && bytes) SP_CUDA_TRY(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return SP_OK;
+    };
+    if ((rc = rowptr(s->A.rp, m, a_row_ptr)) || (rc = rowptr(s->AT.rp, n, at_row_ptr)) ||
+        (rc = copy(a_col_idx, s->A.ci, sizeof(int) * nnz)) || (rc = copy(a_values, s->A.v, sizeof(double) * nnz)) ||
+        (rc = copy(at_col_idx, s->AT.ci, sizeof(int) * nnz)) || (rc = copy(at_values, s->AT.v, sizeof(double) * nnz)) ||
+        (rc = copy(c, s->c, sizeof(double) * n)) || (rc = copy(lc, s->lc, sizeof(double) * m)) ||
+        (rc = copy(uc, s->uc, sizeof(double) * m)) || (rc = copy(lv, s->lv, sizeof(double) * n)) ||
+        (rc = copy(uv, s->uv, sizeof(double) * n)) || (rc = copy(row_scale, s->row_scale, sizeof(double) * m)) ||
+        (rc = copy(col_scale, s->col_scale, sizeof(double) * n)))
+        return rc;
+    if (bound_scale) *bound_scale = s->bound_scale;
+    if (obj_scale) *obj_scale = s->obj_scale;
+    return SP_OK;
+}

@@ -1,0 +1,311 @@
+// solver_kernels.cuh — the fused passes of one PDHG iteration and of its checks.
+//
+// Per iteration the reference runs spmv_t, primal_step, spmv, dual_step and two
+// halpern_steps (crates/saddlepoint-core/src/solver.rs:334-362), six launches and
+// six sweeps over the vectors. Here an iteration is two tile passes:
+//   P (over A'ᵀ rows = columns j): aty_j = (A'ᵀy)_j, then in the epilogue
+//      x_t = clamp(x - τ(c - aty)), x̄ = 2x_t - x, and the Halpern update of x;
+//   D (over A' rows i): (A'x̄)_i, then y_t = y - σ(ax̄ - clamp(ax̄ - y/σ)) and
+//      the Halpern update of y.
+// x_t, y_t and aty are stored only where a check or a restart reads them. Every
+// element is computed with the reference's operations in the reference's order.
+//
+// Iteration roles inside an epoch of E = check_every iterations:
+//   FIRST (i = 0): FUSED, or K0 when the epoch starts at k = 0 (the fixed-point
+//          residual of the anchor is measured, solver.rs:341-346);
+//   MID:   FUSED;
+//   CHECK (i = E-1): writes x_t, y_t, aty and the partial sums of the residual,
+//          KKT and ray statistics; the controller kernel then decides.
+#pragma once
+
+#include "control.cuh"
+#include "tiles.cuh"
+
+namespace sp {
+
+enum Role : int { ROLE_FIRST = 0, ROLE_MID = 1, ROLE_CHECK = 2 };
+
+// Pointers of the device-resident solve.
+struct SolverPtrs {
+    // A' (rows i) and A'ᵀ (rows j)
+    const int *a_rp, *a_ci, *t_rp, *t_ci;
+    const double *a_v, *t_v;
+    const float *a_v32, *t_v32;
+    const int2 *a_tiles, *t_tiles;
+    // problem vectors
+    const double *c, *lc, *uc, *lv, *uv, *pf, *df;
+    // iterates
+    double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty;
+    float *xbar32, *y32;
+    // partial sums per tile
+    double *partP, *partD, *partT, *partP0, *partD0;
+    const DevParams *prm;
+    DevState *st;
+    int mixed;
+};
+
+struct IterScalars {
+    double tau, sigma, w, rho;
+};
+
+__device__ __forceinline__ IterScalars iter_scalars(const SolverPtrs &s, int i) {
+    IterScalars r;
+    const double omega = s.st->omega, eta = s.prm->eta;
+    r.tau = eta / omega;  // solver.rs:333
+    r.sigma = eta * omega;
+    const unsigned long long k = s.st->k + (unsigned long long)i;
+    r.w = (double)(k + 1) / (double)(k + 2);  // solver.rs:360
+    r.rho = s.prm->reflection;
+    return r;
+}
+
+// Whether a pass of precision LO (FP32 SpMV) should run now.
+__device__ __forceinline__ bool precision_matches(const SolverPtrs &s, bool lo) {
+    return lo ? (s.mixed && !s.st->fp64) : (!s.mixed || s.st->fp64);
+}
+
+// ----------------------------------------------------------------------------------
+// P: the primal pass over A'ᵀ. MODE 0 = FUSED, 1 = K0, 2 = CHECK.
+template <bool LO, int MODE>
+struct PrimalPass {
+    using VT = typename std::conditional<LO, float, double>::type;
+    using ST = VT;
+    static constexpr int G = 1;
+    static constexpr int NP = MODE == 2 ? NP_P : (MODE == 1 ? NP_P0 : 0);
+    static constexpr unsigned F32 = LO ? 1u : 0u;
+    const int *rp, *ci;
+    const VT *vals;
+    const int2 *tiles;
+    SolverPtrs s;
+    int i, role;
+    IterScalars sc;
+
+    __device__ bool setup() {
+        if (s.st->done || !precision_matches(s, LO)) return false;
+        int mode = role == ROLE_MID ? 0 : (role == ROLE_CHECK ? 2 : (s.st->k == 0 ? 1 : 0));
+        if (mode != MODE) return false;
+        sc = iter_scalars(s, i);
+        return true;
+    }
+    __device__ __forceinline__ void prod(int c, VT v, ST (&p)[1]) const {
+        if constexpr (LO) p[0] = v * __ldg(s.y32 + c);
+        else p[0] = v * __ldg(s.y + c);
+    }
+    __device__ __forceinline__ void row(int j, const double (&sum)[1], double *part) const {
+        const double aty = sum[0];
+        const double xj = s.x[j];
+        const double t = clampd(xj - sc.tau * (s.c[j] - aty), s.lv[j], s.uv[j]);  // cpu lib.rs:156
+        const double xb = 2.0 * t - xj;                                           // cpu lib.rs:158
+        if constexpr (LO) s.xbar32[j] = (float)xb;
+        else s.xbar[j] = xb;
+        if constexpr (MODE == 0) {
+            s.x[j] = halpern(xj, t, s.xa[j], sc.w, sc.rho);  // solver.rs:361
+        } else {
+            s.xt[j] = t;
+            const double dx = t - xj;  // fixed_point_residual: x_t - x (solver.rs:277)
+            part[0] += dx * dx;
+            if constexpr (MODE == 2) {
+                s.aty[j] = aty;
+                const double cj = s.c[j];
+                const double dxa = t - s.xa[j];  // infeasibility: x_t - x_anchor (solver.rs:302)
+                const double rv = recession_violation(dxa, s.lv[j], s.uv[j]);
+                part[1] += cj * t;       // primal objective c'ᵀx_t
+                part[2] += aty * t;      // step-implied dual objective terms (solver.rs:268-269)
+                part[3] += t * t;
+                part[4] += xj * t;
+                part[5] += rv * rv;      // primal ray: column violations
+                part[6] += dxa * dxa;    // primal ray norm = distance_sq(x_t, x_anchor)
+                part[7] += cj * dxa;     // primal ray objective
+            }
+        }
+    }
+    __device__ void store(int tile, const double *t) const {
+        double *out = MODE == 2 ? s.partP : s.partP0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) out[tile * NP + q] = t[q];
+    }
+};
+
+// ----------------------------------------------------------------------------------
+// D: the dual pass over A'. MODE 0 = FUSED, 1 = K0, 2 = CHECK.
+// FUSED reads the iteration precision's values; K0 and CHECK read FP64 values and
+// form the iteration's own product in the iteration precision from them.
+template <bool LO, int MODE>
+struct DualPass {
+    using VT = typename std::conditional<LO && MODE == 0, float, double>::type;
+    using ST = typename std::conditional<LO && MODE == 0, float, double>::type;
+    static constexpr int G = MODE == 2 ? 4 : (MODE == 1 ? 2 : 1);
+    static constexpr int NP = MODE == 2 ? NP_D : (MODE == 1 ? NP_D0 : 0);
+    static constexpr unsigned F32 = LO ? 1u : 0u;  // slot 0 is the iteration's product
+    const int *rp, *ci;
+    const VT *vals;
+    const int2 *tiles;
+    SolverPtrs s;
+    int i, role;
+    IterScalars sc;
+
+    __device__ bool setup() {
+        if (s.st->done || !precision_matches(s, LO)) return false;
+        int mode = role == ROLE_MID ? 0 : (role == ROLE_CHECK ? 2 : (s.st->k == 0 ? 1 : 0));
+        if (mode != MODE) return false;
+        sc = iter_scalars(s, i);
+        return true;
+    }
+    __device__ __forceinline__ void prod(int c, VT v, ST (&p)[G]) const {
+        if constexpr (LO) p[0] = ST((float)v * __ldg(s.xbar32 + c));
+        else p[0] = v * __ldg(s.xbar + c);
+        if constexpr (MODE >= 1) {
+            const double xtc = __ldg(s.xt + c);
+            p[1] = v * (xtc - __ldg(s.x + c));  // A'(x_t - x)
+            if constexpr (MODE == 2) {
+                p[2] = v * xtc;                      // A' x_t
+                p[3] = v * (xtc - __ldg(s.xa + c));  // A'(x_t - x_anchor)
+            }
+        }
+    }
+    __device__ __forceinline__ void row(int r, const double (&sum)[G], double *part) const {
+        const double a = sum[0], yi = s.y[r];
+        const double v = a - yi / sc.sigma;                                  // cpu lib.rs:171
+        const double yt = yi - sc.sigma * (a - clampd(v, s.lc[r], s.uc[r])); // cpu lib.rs:172
+        if constexpr (MODE == 0) {
+            const double yn = halpern(yi, yt, s.ya[r], sc.w, sc.rho);
+            s.y[r] = yn;
+            if constexpr (LO) s.y32[r] = (float)yn;  // the FP32 shadow the next P pass gathers
+        } else {
+            const double dy = yt - yi;  // fixed_point_residual: y_t - y (solver.rs:278)
+            part[0] += dy * dy;
+            part[1] += dy * sum[1];     // cross term dyᵀ A'(x_t - x)
+            if constexpr (MODE == 1) {
+                const double yn = halpern(yi, yt, s.ya[r], sc.w, sc.rho);
+                s.y[r] = yn;
+                if constexpr (LO) s.y32[r] = (float)yn;
+            } else {
+                s.yt[r] = yt;
+                const double lc = s.lc[r], uc = s.uc[r];
+                const double e = excess(sum[2], lc, uc) * s.pf[r];
+                const double dya = yt - s.ya[r];
+                const double rv = recession_violation(sum[3], lc, uc);
+                const double fb = forbidden(dya, lc, uc);
+                part[2] += e * e;                       // primal residual
+                part[3] += bound_term(yt, lc, uc);      // dual objective: row terms
+                part[4] += rv * rv;                     // primal ray: row violations
+                part[5] += fb * fb;                     // dual ray: row violations
+                part[6] += bound_term(dya, lc, uc);     // dual ray objective: row terms
+                part[7] += dya * dya;                   // dual ray norm = distance_sq(y_t, y_anchor)
+            }
+        }
+    }
+    __device__ void store(int tile, const double *t) const {
+        double *out = MODE == 2 ? s.partD : s.partD0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) out[tile * NP + q] = t[q];
+    }
+};
+
+// ----------------------------------------------------------------------------------
+// T: the check pass over A'ᵀ with y_t and y_t - y_anchor (always FP64).
+struct CheckPassT {
+    using VT = double;
+    using ST = double;
+    static constexpr int G = 2, NP = NP_T;
+    static constexpr unsigned F32 = 0;
+    const int *rp, *ci;
+    const double *vals;
+    const int2 *tiles;
+    SolverPtrs s;
+    int i;
+    double inv_tau;
+
+    __device__ bool setup() {
+        if (s.st->done) return false;
+        inv_tau = 1.0 / iter_scalars(s, i).tau;  // cpu lib.rs:235
+        return true;
+    }
+    __device__ __forceinline__ void prod(int c, double v, double (&p)[2]) const {
+        const double ytc = __ldg(s.yt + c);
+        p[0] = v * ytc;
+        p[1] = v * (ytc - __ldg(s.ya + c));
+    }
+    __device__ __forceinline__ void row(int j, const double (&sum)[2], double *part) const {
+        const double lv = s.lv[j], uv = s.uv[j], df = s.df[j];
+        const double aty_t = sum[0];
+        const double r = s.c[j] - aty_t;
+        const double f = forbidden(r, lv, uv) * df;
+        const double sd = (s.aty[j] - aty_t - (s.xt[j] - s.x[j]) * inv_tau) * df;
+        const double ra = -sum[1];
+        const double fa = forbidden(ra, lv, uv);
+        part[0] += f * f;                   // dual residual
+        part[1] += bound_term(r, lv, uv);   // dual objective: column terms
+        part[2] += sd * sd;                 // step-implied dual residual
+        part[3] += fa * fa;                 // dual ray: column violations
+        part[4] += bound_term(ra, lv, uv);  // dual ray objective: column terms
+    }
+    __device__ void store(int tile, const double *t) const {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) s.partT[tile * NP + q] = t[q];
+    }
+};
+
+// ----------------------------------------------------------------------------------
+// Power iteration on A'ᵀA' (solver.rs:215-242), device-resident.
+struct PowerA {  // tmp = A' (v * s)
+    using VT = double;
+    using ST = double;
+    static constexpr int G = 1, NP = 0;
+    static constexpr unsigned F32 = 0;
+    const int *rp, *ci;
+    const double *vals;
+    const int2 *tiles;
+    const double *v;
+    double *tmp;
+    DevState *st;
+    double scale;
+    __device__ bool setup() {
+        if (st->pi_done) return false;
+        scale = st->pi_scale;
+        return true;
+    }
+    __device__ __forceinline__ void prod(int c, double val, double (&p)[1]) const {
+        p[0] = val * (__ldg(v + c) * scale);  // the gather sees v after `scale(v, s)`
+    }
+    __device__ __forceinline__ void row(int r, const double (&s)[1], double *) const { tmp[r] = s[0]; }
+    __device__ void store(int, const double *) const {}
+};
+
+struct PowerT {  // v = A'ᵀ tmp, partial ‖v‖²
+    using VT = double;
+    using ST = double;
+    static constexpr int G = 1, NP = 1;
+    static constexpr unsigned F32 = 0;
+    const int *rp, *ci;
+    const double *vals;
+    const int2 *tiles;
+    const double *tmp;
+    double *v;
+    double *part;
+    DevState *st;
+    __device__ bool setup() { return !st->pi_done; }
+    __device__ __forceinline__ void prod(int c, double val, double (&p)[1]) const { p[0] = val * __ldg(tmp + c); }
+    __device__ __forceinline__ void row(int r, const double (&s)[1], double *pp) const {
+        v[r] = s[0];
+        pp[0] += s[0] * s[0];
+    }
+    __device__ void store(int tile, const double *t) const { part[tile] = t[0]; }
+};
+
+template <class Op>
+__device__ __forceinline__ bool try_run(Op &op, unsigned char *smem) {
+    if (!op.setup()) return false;
+    tile_body(op, smem);
+    return true;
+}
+
+// Runs the first of the passes whose setup() accepts this launch (the choice is
+// uniform over the grid: it depends only on the device state).
+template <class... Ops>
+__global__ void __launch_bounds__(NT) k_tiles_any(Ops... ops) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    (void)(try_run(ops, smem) || ...);
+}
+
+}  // namespace sp

@@ -1,0 +1,204 @@
+// tiles.cuh — the row-tile CSR SpMV that every matrix pass of the PDHG is built on.
+//
+// A matrix is cut once, at load time, into tiles of consecutive rows holding at
+// most TILE_NNZ nonzeros and TILE_ROWS rows; a row longer than TILE_NNZ gets a
+// tile of its own. One CTA of NT threads processes one tile:
+//   1. stage: the tile's (col, value) pairs are read with coalesced loads, the
+//      gathered vector entries fetched, and the G products per nonzero written
+//      to shared memory;
+//   2. sum: a row of at most SEQ_MAX entries is summed by one thread in column
+//      order (starting from -0.0 like Rust's `Iterator::sum`, so the FP64 result
+//      equals the reference CPU backend's bit for bit); a longer row is summed by
+//      one warp (lane-strided partial sums, then a fixed shuffle tree); a row of
+//      more than TILE_NNZ entries by the whole CTA (fixed tree);
+//   3. epilogue: Op::row() consumes the sums of each row (primal/dual step,
+//      Halpern update, residual terms) and may accumulate NP partial sums, which
+//      the CTA reduces in a fixed order and writes to per-tile slots.
+// Everything is deterministic: the same inputs give the same bits on every run.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace sp {
+
+// Host: cuts rows [0, nrows) into tiles. `rp` has nrows + 1 entries. Tiles that
+// hold a single row longer than TILE_NNZ come first so they start early.
+inline std::vector<int2> build_tiles(const int64_t *rp, int64_t nrows) {
+    std::vector<int2> longs, shorts;
+    int64_t r = 0;
+    while (r < nrows) {
+        int64_t len = rp[r + 1] - rp[r];
+        if (len > TILE_NNZ) {
+            longs.push_back(make_int2((int)r, (int)(r + 1)));
+            ++r;
+            continue;
+        }
+        int64_t r1 = r, nnz = 0;
+        while (r1 < nrows && r1 - r < TILE_ROWS) {
+            int64_t l = rp[r1 + 1] - rp[r1];
+            if (l > TILE_NNZ || nnz + l > TILE_NNZ) break;
+            nnz += l;
+            ++r1;
+        }
+        shorts.push_back(make_int2((int)r, (int)r1));
+        r = r1;
+    }
+    longs.insert(longs.end(), shorts.begin(), shorts.end());
+    return longs;
+}
+
+template <int G, class ST>
+constexpr size_t tile_smem_bytes() {
+    return (size_t)G * TILE_NNZ * sizeof(ST) + (TILE_ROWS + 1) * sizeof(int);
+}
+
+// Sum of products [a, b) of slot q in accumulation type AT, in order, from -0.0.
+template <class AT, class ST>
+__device__ __forceinline__ AT seq_sum(const ST *__restrict__ p, int a, int b) {
+    AT s = AT(-0.0);
+    for (int e = a; e < b; ++e) s += AT(p[e]);
+    return s;
+}
+
+// Lane-strided partial sums then a shuffle tree; lane 0 gets the row sum.
+template <class AT, class ST>
+__device__ __forceinline__ AT warp_row_sum(const ST *__restrict__ p, int a, int b, int lane) {
+    AT s = AT(-0.0);
+    for (int e = a + lane; e < b; e += 32) s += AT(p[e]);
+    return warp_sum_down(s);
+}
+
+template <class Op>
+__device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
+    using VT = typename Op::VT;
+    using ST = typename Op::ST;
+    constexpr int G = Op::G;
+    constexpr int NP = Op::NP;
+    constexpr unsigned F32 = Op::F32;  // bit q set: slot q accumulates in float
+    ST *prod = reinterpret_cast<ST *>(smem);
+    int *srp = reinterpret_cast<int *>(smem + (size_t)G * TILE_NNZ * sizeof(ST));
+    const int *__restrict__ rp = op.rp;
+    const int *__restrict__ ci = op.ci;
+    const VT *__restrict__ vals = op.vals;
+
+    const int2 t = op.tiles[blockIdx.x];
+    const int r0 = t.x, nr = t.y - t.x;
+    const int k0 = rp[r0], nk = rp[t.y] - k0;
+    double part[NP > 0 ? NP : 1];
+#pragma unroll
+    for (int q = 0; q < (NP > 0 ? NP : 1); ++q) part[q] = 0.0;
+
+    if (nk > TILE_NNZ) {
+        // One long row: every thread sums a strided slice, then a fixed tree.
+        float sf[G];
+        double sd[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) { sf[q] = -0.0f; sd[q] = -0.0; }
+        for (int e = threadIdx.x; e < nk; e += NT) {
+            const int k = k0 + e;
+            ST p[G];
+            op.prod(ci[k], vals[k], p);
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                if ((F32 >> q) & 1u) sf[q] += float(p[q]);
+                else sd[q] += double(p[q]);
+            }
+        }
+        double *sh = reinterpret_cast<double *>(smem);
+        double tot[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            // A float slot is reduced in float through the same tree.
+            if ((F32 >> q) & 1u) {
+                float s = warp_sum_down(sf[q]);
+                if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+                __syncthreads();
+                if (threadIdx.x < 32) {
+                    float v = threadIdx.x < NT / 32 ? float(sh[threadIdx.x]) : 0.0f;
+                    v = warp_sum_down(v);
+                    tot[q] = v;
+                }
+                __syncthreads();
+            } else {
+                double s = warp_sum_down(sd[q]);
+                if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+                __syncthreads();
+                if (threadIdx.x < 32) {
+                    double v = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+                    tot[q] = warp_sum_down(v);
+                }
+                __syncthreads();
+            }
+        }
+        if (threadIdx.x == 0) op.row(r0, tot, part);
+    } else {
+        // Stage the products of the tile's nonzeros.
+#pragma unroll 4
+        for (int e = threadIdx.x; e < nk; e += NT) {
+            const int k = k0 + e;
+            ST p[G];
+            op.prod(ci[k], vals[k], p);
+#pragma unroll
+            for (int q = 0; q < G; ++q) prod[q * TILE_NNZ + e] = p[q];
+        }
+        for (int i = threadIdx.x; i <= nr; i += NT) srp[i] = rp[r0 + i] - k0;
+        __syncthreads();
+        // Short rows: one thread per row, in column order.
+        for (int i = threadIdx.x; i < nr; i += NT) {
+            const int a = srp[i], b = srp[i + 1];
+            if (b - a <= SEQ_MAX) {
+                double s[G];
+#pragma unroll
+                for (int q = 0; q < G; ++q)
+                    s[q] = ((F32 >> q) & 1u) ? double(seq_sum<float>(prod + q * TILE_NNZ, a, b))
+                                             : seq_sum<double>(prod + q * TILE_NNZ, a, b);
+                op.row(r0 + i, s, part);
+            }
+        }
+        // Longer rows: one warp per row.
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int i = warp; i < nr; i += NT / 32) {
+            const int a = srp[i], b = srp[i + 1];
+            if (b - a > SEQ_MAX) {
+                double s[G];
+#pragma unroll
+                for (int q = 0; q < G; ++q)
+                    s[q] = ((F32 >> q) & 1u) ? double(warp_row_sum<float>(prod + q * TILE_NNZ, a, b, lane))
+                                             : warp_row_sum<double>(prod + q * TILE_NNZ, a, b, lane);
+                if (lane == 0) op.row(r0 + i, s, part);
+            }
+        }
+    }
+    if constexpr (NP > 0) {
+        __syncthreads();
+        block_sum<NP>(part, reinterpret_cast<double *>(smem));
+        if (threadIdx.x == 0) op.store(blockIdx.x, part);
+    }
+}
+
+// One CTA per tile. Op::setup() reads the device state and returns false when
+// the pass has nothing to do (solve finished, or a role this epoch skips).
+template <class Op>
+__global__ void __launch_bounds__(NT) k_tiles(Op op) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (!op.setup()) return;
+    tile_body(op, smem);
+}
+
+// Mixed form: the same pass in two precisions, chosen per launch from the state
+// (FP32 SpMV until the switch to FP64, then FP64), so one graph serves both.
+template <class OpLo, class OpHi>
+__global__ void __launch_bounds__(NT) k_tiles2(OpLo lo, OpHi hi, const DevState *st) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (st->fp64) {
+        if (!hi.setup()) return;
+        tile_body(hi, smem);
+    } else {
+        if (!lo.setup()) return;
+        tile_body(lo, smem);
+    }
+}
+
+}  // namespace sp
