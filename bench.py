@@ -1,0 +1,570 @@
+#!/usr/bin/env python
+"""Benchmark of the PDHG hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload (N=1): the single large LP — m = 2,000,000 rows, n = 4,000,000 columns,
+40,000,000 nonzeros, column degrees from a Zipf(1.5) law on [2, 5000] rescaled to the
+nonzero total, N(0,1) values, rows/bounds/cost as the random LP recipe (seeded synthetic
+data). A step is one epoch of 64 PDHG iterations (the reference's check interval) with
+its termination/restart check. `value` is PDHG iterations per second of the plain FP64
+form, device-resident (inputs in HBM before the timed region); the mixed FP32-SpMV/FP64-
+state form is reported beside it. `e2e` times the public one-call API (sp_solve) from
+pinned host arrays to the solution back on the host, for K·64 iterations. The matrices
+(≥ 1.2 GB) are far larger than the 126 MB L2, so no flush is needed between steps.
+
+Other workloads (one JSON line each): transport (2000 x 2000 transportation LP),
+batch (the 4096-LP uneven batch, solves/s), serve (Poisson arrivals, p50/p99 latency).
+
+With --gpus N > 1 (launched by torchrun) every rank runs an independent replica of the
+workload on its own GPU ("replicas only": the single-GPU path has no exchange step);
+times are the max over ranks and `value` sums the ranks' work.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ITERS_PER_STEP = 64
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["powerlaw", "transport", "batch", "serve"], default="powerlaw")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the power-law LP's m, n and nnz by this factor (profiling runs only)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+
+class Dist:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            backend = "nccl"
+            try:
+                import torch
+
+                torch.cuda.set_device(self.local)
+            except Exception:
+                backend = "gloo"
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present
+    (a line 'dram_bytes_per_launch <kernel> <bytes>' in profiles/ncu_traffic.txt)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 3 and f[0] == "dram_bytes_per_launch" and f[1] == kernel:
+                return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------ workloads
+
+def powerlaw_lp(seed: int, scale: float = 1.0):
+    import saddlepoint_b200 as sp
+
+    m, n, nnz = (int(round(v * scale)) for v in (2_000_000, 4_000_000, 40_000_000))
+    return sp.generate_powerlaw_lp(seed, m, n, nnz, 1.5, 2, 5000)
+
+
+WORKLOAD_DESC = {
+    "powerlaw": {"workload": "single large LP, power-law columns", "m": 2_000_000, "n": 4_000_000,
+                 "nnz": 40_000_000, "column_degrees": "Zipf(1.5) on [2,5000] rescaled to 40M", "values": "N(0,1)",
+                 "iterations_per_step": ITERS_PER_STEP, "l2": "inputs larger than L2 (no flush)"},
+    "transport": {"workload": "transportation LP 2000 x 2000", "m": 4000, "n": 4_000_000, "nnz": 8_000_000,
+                  "iterations_per_step": ITERS_PER_STEP, "l2": "inputs larger than L2 (no flush)"},
+}
+
+
+def pinned_copy(lp):
+    """The LP's arrays in page-locked host memory (the e2e inputs)."""
+    import numpy as np
+    import torch
+
+    import saddlepoint_b200 as sp
+
+    def pin(a, dt):
+        t = torch.empty(len(a), dtype=dt, pin_memory=True)
+        arr = t.numpy()
+        arr[:] = a
+        return arr, t
+
+    keep = []
+    out = {}
+    for k, dt in [("row_ptr", torch.int64), ("col_idx", torch.int32), ("values", torch.float64), ("c", torch.float64),
+                  ("lc", torch.float64), ("uc", torch.float64), ("lv", torch.float64), ("uv", torch.float64)]:
+        arr, t = pin(getattr(lp, k), dt)
+        keep.append(t)
+        out[k] = arr
+    p = sp.LpProblem(lp.nrows, lp.ncols, out["row_ptr"], out["col_idx"], out["values"], out["c"], out["lc"],
+                     out["uc"], out["lv"], out["uv"], lp.c0, lp.maximize, lp.name)
+    return p, keep
+
+
+def time_form(sp, torch, lp, backend, precision, steps, warmup, dist, device):
+    """Device-resident iterations/s of one precision; returns a dict of measurements."""
+    params = sp.SolverParams(tolerance=1e-12, max_iterations=10**9, precision=precision)
+    solver = sp.Solver(lp, params, backend)
+    stream = torch.cuda.ExternalStream(backend.stream(), device=f"cuda:{device}")
+    solver.run_epochs(warmup)
+    solver.sync()
+    solver.set_timing(4)  # events around every 4th primal/dual launch pair
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    with Clocks(device) as clk:
+        e0.record(stream)
+        solver.run_epochs(steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize(device)
+    ms = e0.elapsed_time(e1)
+    ms_max = dist.max(ms)
+    kern = {}
+    for kid, name in ((0, "primal_pass"), (1, "dual_pass")):
+        n, tot, bpl = solver.kernel_timing(kid)
+        kern[name] = {"launches_timed": n, "avg_ms": tot / max(n, 1), "bytes_per_launch": bpl}
+    info = solver.info()
+    out = {
+        "ms": ms_max, "iters": steps * ITERS_PER_STEP, "kernels": kern, "clocks": clk.summary(),
+        "bytes_per_iteration": solver.bytes_per_iteration(), "setup_s": info.setup_time_s,
+        "norm_estimate": info.norm_estimate, "fp64_from_iteration": int(info.fp64_from_iteration),
+        "scaled": solver.scaled() if precision == sp.Precision.FP64 else None,
+    }
+    solver.close()
+    return out
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import saddlepoint_b200 as sp
+
+    dist = Dist(args.gpus)
+    device = dist.local
+    lp = powerlaw_lp(args.seed, args.scale) if args.workload == "powerlaw" else sp.generate_transport_lp(args.seed)
+    backend = sp.CudaBackend(device)
+    res = {}
+    for prec in (sp.Precision.FP64, sp.Precision.Mixed):
+        res[prec] = time_form(sp, torch, lp, backend, prec, args.steps, args.warmup, dist, device)
+    f64, mix = res[sp.Precision.FP64], res[sp.Precision.Mixed]
+    n = dist.world
+    value = n * f64["iters"] / (f64["ms"] * 1e-3)
+    mixed_value = n * mix["iters"] / (mix["ms"] * 1e-3)
+
+    peak, peak_kind = measured_peak()
+
+    def roofline(meas):
+        k = meas["kernels"]
+        dom = max(k, key=lambda name: k[name]["avg_ms"])
+        d = k[dom]
+        achieved = d["bytes_per_launch"] / (d["avg_ms"] * 1e-3) / 1e9 if d["avg_ms"] > 0 else 0.0
+        return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(dom),
+                "bytes_per_launch": d["bytes_per_launch"], "avg_launch_ms": d["avg_ms"],
+                "launches_timed": d["launches_timed"],
+                "other": {name: {"achieved_gbs": k[name]["bytes_per_launch"] / (k[name]["avg_ms"] * 1e-3) / 1e9
+                                 if k[name]["avg_ms"] > 0 else None, "avg_launch_ms": k[name]["avg_ms"]}
+                          for name in k if name != dom}}
+
+    # e2e: the one-call public API from pinned host memory, K·64 iterations
+    pinned, keep = pinned_copy(lp)
+    stream = torch.cuda.ExternalStream(backend.stream(), device=f"cuda:{device}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = args.steps * ITERS_PER_STEP
+    dist.barrier()
+    torch.cuda.synchronize(device)
+    e0.record(stream)
+    sol = sp.solve(pinned, sp.SolverParams(tolerance=1e-12, max_iterations=iters), backend)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = dist.max(e0.elapsed_time(e1))
+    assert sol.iterations == iters, sol.iterations
+    h2d = 4 * (lp.nrows + 1) + 4 * lp.nnz + 8 * lp.nnz + 8 * (3 * lp.ncols + 2 * lp.nrows)
+    d2h = 8 * (lp.ncols + lp.nrows)
+    e2e = {"value": n * iters / (e2e_ms * 1e-3), "unit": "iter/s", "h2d_bytes_per_step": h2d / args.steps,
+           "d2h_bytes_per_step": d2h / args.steps, "ms_total": e2e_ms, "api": "sp_solve (one call: upload, GPU "
+           "scaling and transpose, power iteration, K*64 PDHG iterations, unscaled solution back)"}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(lp, f64["scaled"], f64["norm_estimate"])
+
+    clocks = f64["clocks"]
+    launches_per_epoch = 2 * ITERS_PER_STEP + 4
+    line = {
+        "metric": "PDHG iter/s (FP64, device-resident)",
+        "value": value,
+        "unit": "iter/s",
+        "n_gpus": n,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": f64["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, see DESIGN.md)",
+        "config": dict(WORKLOAD_DESC[args.workload], parallelism=f"replicas x{n}", seed=args.seed,
+                       **({"scale": args.scale, "m": lp.nrows, "n": lp.ncols, "nnz": lp.nnz} if args.scale != 1.0 else {})),
+        "roofline": roofline(f64),
+        "e2e": e2e,
+        "gpu_launches": launches_per_epoch * args.steps,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "cpu_baseline": cpu,
+        "forms": {
+            "fp64": {"iter_per_s": value, "ms_per_step": f64["ms"] / args.steps,
+                     "gb_per_iteration": f64["bytes_per_iteration"] / 1e9,
+                     "hbm_gbs_whole_iteration": f64["bytes_per_iteration"] * value / n / 1e9},
+            "mixed": {"iter_per_s": mixed_value, "ms_per_step": mix["ms"] / args.steps,
+                      "gb_per_iteration": mix["bytes_per_iteration"] / 1e9,
+                      "hbm_gbs_whole_iteration": mix["bytes_per_iteration"] * mixed_value / n / 1e9,
+                      "roofline": roofline(mix), "clocks": mix["clocks"],
+                      "speedup_vs_fp64": mixed_value / value,
+                      "note": "FP32 SpMV through the timed window (tolerance 1e-12 keeps it from switching)"},
+        },
+        "setup_s": f64["setup_s"],
+    }
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    backend.close()
+    dist.close()
+
+
+def cpu_baseline(lp, scaled, norm_estimate, iters=ITERS_PER_STEP):
+    """The CPU oracle's loop on the same scaled problem (bit-identical to the oracle's own
+    ScaledProblem), one epoch of `iters` iterations, all host threads."""
+    import oracle
+
+    r = oracle.solve_scaled(lp, scaled, tolerance=1e-12, norm_estimate=norm_estimate, stop_after=iters)
+    return {"value": r.iterations / r.solve_time, "unit": "iter/s", "cores": oracle.get_threads(),
+            "kind": "port", "sample": f"{r.iterations} PDHG iterations (one epoch incl. its check) of the same "
+            f"LP on the C restatement of the reference's CPU backend, {r.solve_time:.2f} s"}
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the path (the C restatement; the Rust
+    crate cannot be built here) on this arm's workload, metric and unit."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import oracle
+
+    t0 = time.time()
+    lp = powerlaw_lp(args.seed, args.scale)
+    s = oracle.scaled_problem(lp)
+    setup_s = time.time() - t0
+    # ‖A'‖₂ only sets the step size, not the cost of an iteration: a fixed value keeps
+    # the 200 power-iteration SpMVs out of the sample.
+    norm = 1.0
+    probe = oracle.solve_scaled(lp, s, tolerance=1e-12, norm_estimate=norm, stop_after=2)
+    t_it = max(probe.solve_time / 2, 1e-3)
+    # steps of `per_step` iterations, run as one continuous loop (checks every 64
+    # iterations as in the reference), sized so the timed part stays near two minutes
+    per_step = int(max(1, min(ITERS_PER_STEP, 120.0 / max(args.steps, 1) / t_it)))
+    oracle.solve_scaled(lp, s, tolerance=1e-12, norm_estimate=norm, stop_after=max(1, args.warmup) * per_step)
+    r = oracle.solve_scaled(lp, s, tolerance=1e-12, norm_estimate=norm, stop_after=args.steps * per_step)
+    tot_it, tot_s = r.iterations, r.solve_time
+    value = tot_it / tot_s
+    sample = (f"{args.steps} steps of {per_step} PDHG iterations ({tot_it} in one loop, a check every 64) on the C "
+              f"restatement of the reference's CPU backend, {oracle.get_threads()} threads; "
+              f"generation and scaling ({setup_s:.0f} s) untimed")
+    line = {
+        "impl": "reference", "metric": "PDHG iter/s (FP64, device-resident)", "value": value, "unit": "iter/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, see DESIGN.md)",
+        "config": dict(WORKLOAD_DESC["powerlaw"], parallelism="host threads", seed=args.seed),
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": oracle.get_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def batch_instances(seed: int, count: int):
+    """The uneven batch: per instance m log-uniform in [50, 2000], n = 2m, 3-8 nonzeros
+    per column, built like the random LP recipe from a per-instance seed."""
+    import math
+
+    import numpy as np
+
+    import saddlepoint_b200 as sp
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        m = int(round(math.exp(rng.uniform(math.log(50), math.log(2000)))))
+        out.append(sp.generate_random_lp(seed * 1_000_003 + i, m, 2 * m, (3, 8)))
+    return out
+
+
+def run_batch(args):
+    """Solves/s of the batched persistent kernel on the 4096-LP uneven batch (tol 1e-6),
+    against the plain device-resident form solving instances one at a time."""
+    import numpy as np
+    import torch
+
+    import saddlepoint_b200 as sp
+
+    dist = Dist(args.gpus)
+    count = 4096
+    lps = batch_instances(args.seed, count)
+    backend = sp.CudaBackend(dist.local)
+    out = {}
+    for prec in (sp.Precision.FP64, sp.Precision.Mixed):
+        b = sp.BatchSolver(lps, sp.SolverParams(tolerance=1e-6, precision=prec), backend)
+        res, _ = b.solve()  # warm-up
+        times = []
+        dist.barrier()
+        with Clocks(dist.local) as clk:
+            for _ in range(max(1, min(args.steps, 3))):
+                res, t = b.solve()
+                times.append(t)
+        t_max = dist.max(max(times))
+        st = np.array([r.status for r in res])
+        its = np.array([r.iterations for r in res])
+        out[prec] = {"solves_per_s": dist.world * count / t_max, "s_per_batch": t_max,
+                     "optimal": int((st == 0).sum()), "iterations_median": float(np.median(its)),
+                     "iterations_max": int(its.max()), "clocks": clk.summary()}
+        b.close()
+    # the plain form: one device-resident solve per instance, on a spread sample
+    sample = lps[:: count // 32]
+    t0 = time.time()
+    plain_ok = 0
+    for lp in sample:
+        s = sp.solve(lp, sp.SolverParams(tolerance=1e-6), backend)
+        plain_ok += int(s.status == sp.Status.Optimal)
+    plain_s = time.time() - t0
+    plain = len(sample) / plain_s
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        t0 = time.time()
+        k = 0
+        for lp in sample[:8]:
+            oracle.solve(lp, tolerance=1e-6)
+            k += 1
+        cpu = {"value": k / (time.time() - t0), "unit": "solves/s", "cores": oracle.get_threads(), "kind": "port",
+               "sample": f"{k} instances of the batch solved one after another by the C restatement (serial below "
+               "32768 elements, like the reference)"}
+    f64 = out[sp.Precision.FP64]
+    line = {
+        "metric": "batched solves/s at 1e-6 rel KKT (4096 uneven LPs)", "value": f64["solves_per_s"],
+        "unit": "solves/s", "n_gpus": dist.world, "steps": max(1, min(args.steps, 3)), "warmup": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "4096 LPs, m log-uniform [50,2000], n=2m, 3-8 nnz/col", "tolerance": 1e-6,
+                   "parallelism": f"replicas x{dist.world}"},
+        "forms": {"fp64": f64, "mixed": out[sp.Precision.Mixed],
+                  "plain_device_solve": {"solves_per_s": plain, "sample": len(sample), "optimal": plain_ok},
+                  "batched_over_plain": f64["solves_per_s"] / plain},
+        "cpu_baseline": cpu, "gpu_launches": 1,
+        "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    backend.close()
+    dist.close()
+
+
+def run_serve(args):
+    """The serving loop under Poisson arrivals (λ = 200/s) of random LPs with nnz
+    log-uniform in [1e3, 1e7] (n = nnz/5, m = n/2), tolerance 1e-6: p50/p99 time to
+    solution and solves/s, FP64 and mixed."""
+    import math
+    import threading
+
+    import numpy as np
+
+    import saddlepoint_b200 as sp
+
+    dist = Dist(args.gpus)
+    nreq = max(8, min(args.steps, 400))
+    rng = np.random.default_rng(args.seed)
+    lps = []
+    for i in range(nreq):
+        nnz = math.exp(rng.uniform(math.log(1e3), math.log(1e7)))
+        n = max(10, int(nnz / 5))
+        lps.append(sp.generate_random_lp(args.seed * 7919 + i, max(5, n // 2), n, (5, 5)))
+    gaps = rng.exponential(1.0 / 200.0, size=nreq)
+    backend = sp.CudaBackend(dist.local)
+    forms = {}
+    for prec in (sp.Precision.FP64, sp.Precision.Mixed):
+        srv = sp.Server(budget_bytes=150e9, max_inflight=8, batch_max_nnz=50_000,
+                        params=sp.SolverParams(tolerance=1e-6, max_iterations=200_000, precision=prec),
+                        backend=backend)
+        results = []
+
+        def collect():
+            while len(results) < nreq:
+                r = srv.poll(timeout=1.0)
+                if r is not None:
+                    results.append(r)
+
+        th = threading.Thread(target=collect)
+        th.start()
+        t0 = time.time()
+        with Clocks(dist.local) as clk:
+            due = t0
+            for lp, g in zip(lps, gaps):
+                due += g
+                delay = due - time.time()
+                if delay > 0:
+                    time.sleep(delay)
+                srv.submit(lp)
+            th.join()
+        wall = time.time() - t0
+        srv.close()
+        lat = np.array([r.total_s for r in results])
+        forms[prec] = {"solves_per_s": nreq / wall, "p50_s": float(np.percentile(lat, 50)),
+                       "p99_s": float(np.percentile(lat, 99)),
+                       "optimal": int(sum(r.status == 0 for r in results)), "requests": nreq,
+                       "queue_p50_s": float(np.median([r.queue_s for r in results])), "clocks": clk.summary()}
+    f64 = forms[sp.Precision.FP64]
+    line = {
+        "metric": "serving solves/s and p50/p99 time to 1e-6 (Poisson 200/s)", "value": f64["solves_per_s"],
+        "unit": "solves/s", "n_gpus": dist.world, "steps": nreq, "warmup": 0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": "Poisson arrivals 200/s, nnz log-uniform [1e3,1e7], n=nnz/5, m=n/2",
+                   "budget_bytes": 150e9, "max_inflight": 8, "batch_max_nnz": 50_000, "requests": nreq},
+        "forms": {"fp64": f64, "mixed": forms[sp.Precision.Mixed]},
+        "p50_s": f64["p50_s"], "p99_s": f64["p99_s"],
+        "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    backend.close()
+    dist.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        if args.workload != "powerlaw":
+            print(json.dumps({"impl": "reference", "unavailable": "reference arm is defined for the default workload"}))
+            return
+        run_reference(args)
+        return
+    if args.workload in ("powerlaw", "transport"):
+        run_ours(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    else:
+        run_serve(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -414,6 +414,40 @@ def solve(p, params: SolverParams | None = None, **kw) -> OracleSolution:
     return out
 
 
+def solve_scaled(p, s, params: SolverParams | None = None, norm_estimate: float = 0.0, stop_after: int = 0,
+                 **kw) -> OracleSolution:
+    """Solver::run (solver.rs:311-438) on a given ScaledProblem ``s`` (any object with the
+    attributes of ``Scaled``); ``norm_estimate`` > 0 replaces estimate_norm; ``stop_after`` > 0
+    ends the loop after that many iterations without forcing a check. Used to time the loop
+    alone on a large problem without the serial scaling passes."""
+    L = lib()
+    L.or_solve_scaled.argtypes = [C.POINTER(Lp), C.POINTER(ScaledC), C.POINTER(SolverParams), dbl, u64,
+                                  C.POINTER(Solution)]
+    view = _LpView(p)
+    m, n = int(p.nrows), int(p.ncols)
+    keep = [_i64(s.a[0]), _i64(s.a[1]), _f64(s.a[2]), _i64(s.at[0]), _i64(s.at[1]), _f64(s.at[2])]
+    vecs = [_f64(v) for v in (s.c, s.lc, s.uc, s.lv, s.uv, s.row_scale, s.col_scale)]
+    cs = ScaledC()
+    cs.a = Csr(m, n, len(keep[2]), _pi(keep[0]), _pi(keep[1]), _pd(keep[2]))
+    cs.at = Csr(n, m, len(keep[5]), _pi(keep[3]), _pi(keep[4]), _pd(keep[5]))
+    cs.c, cs.lc, cs.uc, cs.lv, cs.uv, cs.row_scale, cs.col_scale = [_pd(v) for v in vecs]
+    cs.bound_scale, cs.obj_scale = float(s.bound_scale), float(s.obj_scale)
+    prm = params if params is not None else default_params(**kw)
+    sol = Solution()
+    rc = L.or_solve_scaled(C.byref(view.s), C.byref(cs), C.byref(prm), float(norm_estimate), int(stop_after),
+                           C.byref(sol))
+    if rc != 0:
+        raise RuntimeError(f"oracle solve failed ({rc})")
+    out = OracleSolution(
+        status=STATUS[sol.status], x=_arr(sol.x, n), y=_arr(sol.y, m), objective=sol.objective,
+        dual_objective=sol.dual_objective, primal_residual=sol.primal_residual, dual_residual=sol.dual_residual,
+        gap=sol.gap, iterations=int(sol.iterations), restarts=int(sol.restarts), solve_time=sol.solve_time_s,
+        norm_estimate=sol.norm_estimate,
+    )
+    L.or_solution_free(C.byref(sol))
+    return out
+
+
 def check(p, x, y) -> KktReport:
     """saddlepoint_check::check (crates/saddlepoint-check/src/lib.rs:62-118)."""
     L = lib()

@@ -976,6 +976,7 @@ typedef struct {
     or_cpu_problem dev;
     int64_t m, n;
     double *x, *y, *x_t, *y_t, *x_bar, *x_anchor, *y_anchor, *ax, *aty, *tmp_n, *tmp_m, *tmp_m2, *c;
+    int owns_scaled;
 } solver_t;
 
 /* Solver::estimate_norm (solver.rs:215-242). */
@@ -1075,11 +1076,28 @@ static void solver_free(solver_t *s) {
                    s->ax, s->aty, s->tmp_n, s->tmp_m, s->tmp_m2, s->c};
     for (size_t i = 0; i < sizeof v / sizeof v[0]; ++i) free(v[i]);
     or_cpu_free(&s->dev);
-    or_scaled_free(&s->scaled);
+    if (s->owns_scaled) or_scaled_free(&s->scaled);
 }
+
+static int solve_impl(const or_lp *problem, const or_scaled *given, const or_solver_params *p, double norm_override,
+                      uint64_t stop_after, or_solution *out);
 
 /* solve (solver.rs:154-157) = validate + Solver::new (:185-212) + Solver::run (:311-438). */
 int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) {
+    return solve_impl(problem, NULL, p, 0.0, 0, out);
+}
+
+/* Solver::run on an already scaled problem (borrowed), for timing the loop alone;
+ * norm_override > 0 replaces estimate_norm's result; stop_after > 0 ends the loop
+ * after that many iterations without forcing a check (checks stay every
+ * check_every iterations, the reference's cadence). */
+int or_solve_scaled(const or_lp *problem, const or_scaled *scaled, const or_solver_params *p, double norm_override,
+                    uint64_t stop_after, or_solution *out) {
+    return solve_impl(problem, scaled, p, norm_override, stop_after, out);
+}
+
+static int solve_impl(const or_lp *problem, const or_scaled *given, const or_solver_params *p, double norm_override,
+                      uint64_t stop_after, or_solution *out) {
     memset(out, 0, sizeof *out);
     if (or_lp_validate(problem) != OR_OK) return OR_ERR_PROBLEM;
     solver_t S;
@@ -1089,7 +1107,13 @@ int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) 
     s->params = p;
     s->m = problem->a.nrows;
     s->n = problem->a.ncols;
-    if (or_scaled_new(problem, &p->scaling, &s->scaled) != OR_OK) return OR_ERR_ALLOC;
+    if (given) {
+        s->scaled = *given;
+        s->owns_scaled = 0;
+    } else {
+        if (or_scaled_new(problem, &p->scaling, &s->scaled) != OR_OK) return OR_ERR_ALLOC;
+        s->owns_scaled = 1;
+    }
     or_cpu_load(&s->scaled, &s->dev);
     int64_t m = s->m, n = s->n;
     s->x = dfill(n, 0.0);
@@ -1108,8 +1132,8 @@ int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) 
     memcpy(s->c, s->scaled.c, sizeof(double) * n);
 
     double start = now_s();
-    double norm_est;
-    int rc = estimate_norm(s, &norm_est);
+    double norm_est = norm_override;
+    int rc = norm_override > 0.0 ? OR_OK : estimate_norm(s, &norm_est);
     if (rc != OR_OK) {
         solver_free(s);
         return rc;
@@ -1126,7 +1150,7 @@ int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) 
     double anchor_residual = INFINITY, prev_residual = INFINITY;
     int64_t trace_cap = 0;
     int status;
-    kkt_t kk;
+    kkt_t kk = {0.0, 0.0, 0.0, 0.0};
     for (;;) {
         double tau = eta / omega, sigma = eta * omega;
         or_cpu_spmv_t(&s->dev, s->y, s->aty);
@@ -1156,7 +1180,13 @@ int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) 
         or_cpu_halpern_step(s->x, s->x_t, s->x_anchor, w, p->reflection, n);
         or_cpu_halpern_step(s->y, s->y_t, s->y_anchor, w, p->reflection, m);
         k += 1;
-        if (!check) continue;
+        if (!check) {
+            if (stop_after && total >= stop_after) {  /* a timing sample ends without a forced check */
+                status = OR_ITERATION_LIMIT;
+                break;
+            }
+            continue;
+        }
 
         or_check_record rec;
         memset(&rec, 0, sizeof rec);
@@ -1210,6 +1240,10 @@ int or_solve(const or_lp *problem, const or_solver_params *p, or_solution *out) 
         rec.omega = omega;
         rec.k_after = k;
         push_trace(out, &trace_cap, rec);
+        if (stop_after && total >= stop_after) {
+            status = OR_ITERATION_LIMIT;
+            break;
+        }
     }
     out->x = dalloc(n);
     out->y = dalloc(m);

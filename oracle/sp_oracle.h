@@ -168,6 +168,10 @@ or_ray_stats or_cpu_dual_ray_stats(const or_cpu_problem *p, const double *dy, co
 /* ---- solver (solver.rs:154-480) ------------------------------------------- */
 void or_solver_params_default(or_solver_params *p);
 int or_solve(const or_lp *p, const or_solver_params *params, or_solution *out);
+/* Solver::run on a given ScaledProblem (borrowed); norm_override > 0 skips estimate_norm;
+ * stop_after > 0 ends the loop after that many iterations without forcing a check. */
+int or_solve_scaled(const or_lp *p, const or_scaled *scaled, const or_solver_params *params, double norm_override,
+                    uint64_t stop_after, or_solution *out);
 void or_solution_free(or_solution *s);
 /* PidState::update (solver.rs:459-479), exposed for its unit tests. */
 typedef struct { double integral; double prev_error; int has_prev; double best_weight, best_balance; } or_pid;

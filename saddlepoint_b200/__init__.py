@@ -251,31 +251,48 @@ class ScaledProblem:
         return ys * self.row_scale / self.obj_scale
 
 
-class Vector:
+class _Handle:
+    """A native object that belongs to a backend's context. The backend keeps a weak
+    reference to each, so closing the backend frees its objects first and a handle
+    never outlives the context it was made on."""
+
+    _free = ""
+
+    def _attach(self, backend: "CudaBackend", handle):
+        self.backend, self.h = backend, handle
+        backend._children.add(self)
+
+    def close(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.h = None
+            getattr(library(), self._free)(h)
+
+    def __del__(self):
+        self.close()
+
+
+class Vector(_Handle):
     """A device vector owned by the backend (Backend::Vector)."""
 
+    _free = "sp_vec_free"
+
     def __init__(self, backend: "CudaBackend", handle, n: int):
-        self.backend, self.h, self.n = backend, handle, n
+        self.n = n
+        self._attach(backend, handle)
 
     def __len__(self):
         return self.n
 
-    def __del__(self):
-        if getattr(self, "h", None):
-            library().sp_vec_free(self.h)
-            self.h = None
 
-
-class Problem:
+class Problem(_Handle):
     """The scaled problem on the device (Backend::Problem)."""
 
-    def __init__(self, handle, m: int, n: int):
-        self.h, self.m, self.n = handle, m, n
+    _free = "sp_problem_free"
 
-    def __del__(self):
-        if getattr(self, "h", None):
-            library().sp_problem_free(self.h)
-            self.h = None
+    def __init__(self, backend: "CudaBackend", handle, m: int, n: int):
+        self.m, self.n = m, n
+        self._attach(backend, handle)
 
 
 class CudaBackend:
@@ -286,15 +303,20 @@ class CudaBackend:
     """
 
     def __init__(self, ordinal: int = 0):
+        import weakref
+
         lib = library()
         h = C.c_void_p()
         rc = lib.sp_ctx_create(ordinal, C.byref(h))
         if rc != L.SP_OK:
             raise BackendError(rc, f"no usable CUDA device {ordinal}")
         self.lib, self.h = lib, h
+        self._children = weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
+            for child in list(self._children):
+                child.close()
             self.lib.sp_ctx_destroy(self.h)
             self.h = None
 
@@ -323,7 +345,7 @@ class CudaBackend:
         vecs = [_f64(v) for v in (s.c, s.lc, s.uc, s.lv, s.uv, s.primal_residual_factors(), s.dual_residual_factors())]
         h = C.c_void_p()
         self._check(self.lib.sp_problem_load(self.h, C.byref(A), C.byref(AT), *[_pd(v) for v in vecs], C.byref(h)))
-        return Problem(h, s.nrows, s.ncols)
+        return Problem(self, h, s.nrows, s.ncols)
 
     def upload(self, data) -> Vector:
         d = _f64(data)
@@ -416,28 +438,21 @@ def _backend(b: Optional[CudaBackend]) -> CudaBackend:
     return _default_backend
 
 
-class Solver:
+class Solver(_Handle):
     """A device-resident solve of one LP (scaling, ‖A'‖₂ and iterates stay on the GPU)."""
 
+    _free = "sp_solver_free"
+
     def __init__(self, problem, params: Optional[SolverParams] = None, backend: Optional[CudaBackend] = None):
-        self.backend = _backend(backend)
+        backend = _backend(backend)
         self.problem = LpProblem.from_any(problem)
         self.params = params or SolverParams()
         view = _LpView(self.problem)
         cp = self.params.to_c()
         h = C.c_void_p()
-        self.lib = self.backend.lib
-        self.backend._check(self.lib.sp_solver_create(self.backend.h, C.byref(view.s), C.byref(cp), C.byref(h)),
-                            SolveError)
-        self.h = h
-
-    def close(self):
-        if getattr(self, "h", None):
-            self.lib.sp_solver_free(self.h)
-            self.h = None
-
-    def __del__(self):
-        self.close()
+        self.lib = backend.lib
+        backend._check(self.lib.sp_solver_create(backend.h, C.byref(view.s), C.byref(cp), C.byref(h)), SolveError)
+        self._attach(backend, h)
 
     def _c(self, rc):
         self.backend._check(rc, SolveError)

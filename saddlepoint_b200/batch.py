@@ -16,6 +16,17 @@ def _pkg():
     return saddlepoint_b200
 
 
+from . import _Handle  # noqa: E402  (the package defines it before importing this module)
+
+
+class _BatchHandle(_Handle):
+    _free = "sp_batch_free"
+
+
+class _ServerHandle(_Handle):
+    _free = "sp_server_destroy"
+
+
 @dataclass
 class BatchResult:
     status: int  # Status value, or negative for a numerical breakdown
@@ -39,25 +50,22 @@ class BatchSolver:
 
     def __init__(self, problems: list, params=None, backend=None):
         sp = _pkg()
-        self.backend = sp._backend(backend)
-        self.lib = self.backend.lib
+        backend = sp._backend(backend)
+        self.lib = backend.lib
         self.problems = [sp.LpProblem.from_any(p) for p in problems]
-        self._views = [sp._LpView(p) for p in self.problems]
-        arr = (L.Lp * len(self._views))(*[v.s for v in self._views])
+        views = [sp._LpView(p) for p in self.problems]
+        arr = (L.Lp * len(views))(*[v.s for v in views])
         cp = (params or sp.SolverParams()).to_c()
         h = C.c_void_p()
-        self.backend._check(self.lib.sp_batch_create(self.backend.h, arr, len(self._views), C.byref(cp), C.byref(h)),
-                            sp.SolveError)
-        self.h = h
+        backend._check(self.lib.sp_batch_create(backend.h, arr, len(views), C.byref(cp), C.byref(h)), sp.SolveError)
+        self._handle = _BatchHandle()
+        self._handle._attach(backend, h)
+        self.backend, self.h = backend, h
         self.count = len(self.problems)
 
     def close(self):
-        if getattr(self, "h", None):
-            self.lib.sp_batch_free(self.h)
-            self.h = None
-
-    def __del__(self):
-        self.close()
+        self._handle.close()
+        self.h = None
 
     def solve(self):
         res = (L.BatchResult * self.count)()
@@ -104,13 +112,15 @@ class Server:
     def __init__(self, budget_bytes: float = 150e9, max_inflight: int = 8, batch_max_nnz: int = 50_000,
                  params=None, backend=None):
         sp = _pkg()
-        self.backend = sp._backend(backend)
-        self.lib = self.backend.lib
+        backend = sp._backend(backend)
+        self.lib = backend.lib
         cfg = L.ServerConfig(float(budget_bytes), int(max_inflight), int(batch_max_nnz))
         cp = (params or sp.SolverParams()).to_c()
         h = C.c_void_p()
-        self.backend._check(self.lib.sp_server_create(self.backend.h, C.byref(cfg), C.byref(cp), C.byref(h)))
-        self.h = h
+        backend._check(self.lib.sp_server_create(backend.h, C.byref(cfg), C.byref(cp), C.byref(h)))
+        self._handle = _ServerHandle()
+        self._handle._attach(backend, h)
+        self.backend, self.h = backend, h
         self._shapes = {}
 
     def submit(self, problem) -> int:
@@ -138,12 +148,8 @@ class Server:
                             int(r.footprint_bytes), x[:n].copy(), y[:m].copy())
 
     def close(self):
-        if getattr(self, "h", None):
-            self.lib.sp_server_destroy(self.h)
-            self.h = None
-
-    def __del__(self):
-        self.close()
+        self._handle.close()
+        self.h = None
 
     @staticmethod
     def footprint(nrows: int, ncols: int, nnz: int, precision: int = 0) -> int:

@@ -312,6 +312,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         st.prev_residual = INFINITY;
         st.pid_best_weight = st.omega;
         st.pid_best_balance = INFINITY;
+        st.mx_best = INFINITY;
         if (numerical) {
             st.done = 1;
             st.error = ERR_NUMERICAL_POWER;

@@ -118,7 +118,14 @@ struct DevState {
     double pi_scale, pi_lambda;
     int pi_done, pi_iters;
     unsigned long long trace_len;
+    // mixed form: best relative KKT error of the FP32 phase and checks since it improved
+    double mx_best;
+    int mx_since, pad1;
 };
+
+// Mixed form: checks without a 10% gain in the relative KKT error after which the
+// FP32 phase is taken to have stalled at its precision and the SpMV moves to FP64.
+constexpr int MIXED_STALL_CHECKS = 40;
 
 enum : int { ERR_NONE = 0, ERR_NUMERICAL_POWER = 1, ERR_NUMERICAL_ITERATES = 2 };
 

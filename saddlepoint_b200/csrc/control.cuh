@@ -127,11 +127,18 @@ __device__ __forceinline__ void check_decide(DevState *st, const DevParams *p, c
         rec->k_after = k;
         return;
     }
-    // Mixed form: move the SpMV to FP64 once the relative KKT error is small.
+    // Mixed form: move the SpMV to FP64 once the relative KKT error is small, or
+    // once the FP32 phase stops making progress (it has reached its precision).
     if (p->mixed && !st->fp64) {
         const double rel = fmax(fmax(primal_res / (1.0 + p->b_norm), dual_res / (1.0 + p->c_norm)),
                                 fabs(primal_obj - dual_obj) / (1.0 + fabs(primal_obj) + fabs(dual_obj)));
-        if (rel < p->mixed_switch_tolerance) {
+        if (rel < 0.9 * st->mx_best) {
+            st->mx_best = rel;
+            st->mx_since = 0;
+        } else {
+            st->mx_since += 1;
+        }
+        if (rel < p->mixed_switch_tolerance || st->mx_since >= MIXED_STALL_CHECKS) {
             st->fp64 = 1;
             st->fp64_from = total + 1;
         }

@@ -784,6 +784,7 @@ extern "C" int sp_solver_reset(sp_solver *s) {
     h.pid_best_weight = h.omega;  // PidState::new (solver.rs:453-455)
     h.pid_best_balance = INFINITY;
     h.pi_done = 1;
+    h.mx_best = INFINITY;
     *s->h_st = h;
     SP_CUDA_TRY(cudaMemcpyAsync(s->d_st, s->h_st, sizeof(DevState), cudaMemcpyHostToDevice, st));
     SP_CUDA_TRY(cudaStreamSynchronize(st));

@@ -110,7 +110,9 @@ def test_restart_trace_matches_cpu(name, gpu_backend):
     for a, b in zip(tg, tr):
         assert a["total"] == b["total"] and a["restarted"] == b["restarted"] and a["k_after"] == b["k_after"]
         assert math.isclose(a["omega"], b["omega"], rel_tol=1e-9)
-        assert math.isclose(a["residual"], b["residual"], rel_tol=1e-9, abs_tol=1e-300)
+        # r² is a difference of the metric's terms, so its rounding error is relative to
+        # those terms, not to r: compare loosely (the decisions above are compared exactly)
+        assert math.isclose(a["residual"], b["residual"], rel_tol=1e-6, abs_tol=1e-300)
 
 
 def tiny():
