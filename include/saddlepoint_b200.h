@@ -283,6 +283,27 @@ int64_t sp_server_footprint(int64_t nrows, int64_t ncols, int64_t nnz, int preci
 void sp_server_destroy(sp_server *s);
 
 /* ========================================================================
+ * Allocation-free reduction. No counterpart in the reference.
+ * ======================================================================== */
+
+/* Maximum length sp_dot_noalloc accepts: its fixed scratch holds one partial sum
+ * per 2048 elements, 32768 of them (256 KiB per GPU, held until process exit). */
+#define SP_NOALLOC_DOT_MAX_N 67108864LL
+
+/* *result = aᵀb for device arrays a and b of n doubles, enqueued on `stream` (a
+ * cudaStream_t; NULL for the default stream); `result` is a device pointer. For
+ * callers that cannot allocate device memory where they need the reduction (inside
+ * stream capture, under their own pool allocator, in a loop that must not
+ * synchronise on cudaMalloc/cudaFree): it allocates nothing and needs no context.
+ * Its two-stage reduction keeps its partial sums in a static device array instead;
+ * n > SP_NOALLOC_DOT_MAX_N returns SP_ERR_TOO_LARGE and launches nothing. The
+ * first call on each device looks up that array's address (cudaGetSymbolAddress);
+ * make that first call before any stream capture. All calls share the array, so
+ * calls that overlap on the GPU (different streams, no ordering between them)
+ * race; calls on one stream are safe. Returns SP_OK or an SP_ERR_* code. */
+int sp_dot_noalloc(const double *a, const double *b, int64_t n, double *result, void *stream);
+
+/* ========================================================================
  * Synthetic LP generators (seeded; see DESIGN.md for the exact recipes).
  * ======================================================================== */
 

@@ -159,6 +159,7 @@ SIGNATURES = [
     ("sp_server_poll", cint, [VP, dbl, C.POINTER(ServerResult), PD, i64, PD, i64, C.POINTER(cint)]),
     ("sp_server_footprint", i64, [i64, i64, i64, cint]),
     ("sp_server_destroy", None, [VP]),
+    ("sp_dot_noalloc", cint, [VP, VP, i64, VP, VP]),
     ("sp_generate", cint, [C.POINTER(GenParams), C.POINTER(Lp)]),
     ("sp_lp_release", None, [C.POINTER(Lp)]),
 ]
