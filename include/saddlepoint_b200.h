@@ -241,7 +241,8 @@ typedef struct {
     int status;
     double objective, dual_objective, primal_residual, dual_residual, gap;
     uint64_t iterations, restarts;
-    int lanes_per_row; /* SpMV variant the tuner chose: lanes cooperating on one row */
+    int lanes_per_row; /* SpMV variant the tuner chose: 0 = staged tiles (the single-LP passes);
+                          otherwise lane groups, 100 * (lanes per row of A') + (lanes per row of A'ᵀ) */
 } sp_batch_result;
 
 /* Scales and uploads `count` LPs into one packed arena. */

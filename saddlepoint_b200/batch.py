@@ -37,8 +37,12 @@ class BatchResult:
     gap: float
     iterations: int
     restarts: int
-    lanes_a: int  # lanes per row the tuner picked for A'
+    lanes_a: int  # lanes per row the tuner picked for A' (0: the staged-tile variant)
     lanes_t: int  # ... and for A'ᵀ
+
+    @property
+    def variant(self) -> str:
+        return "tiles" if self.lanes_a == 0 and self.lanes_t == 0 else "lanes"
 
 
 class BatchSolver:

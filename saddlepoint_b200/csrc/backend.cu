@@ -33,12 +33,14 @@ struct StoreOp {  // out = A x (Backend::spmv / spmv_t)
     static constexpr unsigned F32 = 0;
     const int *rp, *ci;
     const double *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     const double *x;
     double *out;
+    struct Pre {};
     __device__ bool setup() { return true; }
+    __device__ __forceinline__ Pre pre(int) const { return {}; }
     __device__ __forceinline__ void prod(int c, double v, double (&p)[1]) const { p[0] = v * __ldg(x + c); }
-    __device__ __forceinline__ void row(int r, const double (&s)[1], double *) const { out[r] = s[0]; }
+    __device__ __forceinline__ void row(int r, const double (&s)[1], double *, const Pre &) const { out[r] = s[0]; }
     __device__ void store(int, const double *) const {}
 };
 
@@ -374,20 +376,20 @@ int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32) {
         if (i > 0 && h->row_ptr[i] < h->row_ptr[i - 1]) return fail(SP_ERR_INVALID, "CSR row_ptr not monotone");
         rp32[i] = (int)h->row_ptr[i];
     }
-    std::vector<int2> tiles = build_tiles(h->row_ptr, h->nrows);
+    std::vector<Tile> tiles = build_tiles(h->row_ptr, h->nrows);
     d->ntiles = (int)tiles.size();
     size_t nz = (size_t)std::max<int64_t>(h->nnz, 1);
     SP_CUDA_TRY(cudaMalloc(&d->rp, sizeof(int) * (h->nrows + 1)));
     SP_CUDA_TRY(cudaMalloc(&d->ci, sizeof(int) * nz));
     SP_CUDA_TRY(cudaMalloc(&d->v, sizeof(double) * nz));
-    SP_CUDA_TRY(cudaMalloc(&d->tiles, sizeof(int2) * std::max<size_t>(tiles.size(), 1)));
+    SP_CUDA_TRY(cudaMalloc(&d->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
     SP_CUDA_TRY(cudaMemcpyAsync(d->rp, rp32.data(), sizeof(int) * (h->nrows + 1), cudaMemcpyHostToDevice, ctx->stream));
     if (h->nnz) {
         SP_CUDA_TRY(cudaMemcpyAsync(d->ci, h->col_idx, sizeof(int) * h->nnz, cudaMemcpyHostToDevice, ctx->stream));
         SP_CUDA_TRY(cudaMemcpyAsync(d->v, h->values, sizeof(double) * h->nnz, cudaMemcpyHostToDevice, ctx->stream));
     }
     if (!tiles.empty())
-        SP_CUDA_TRY(cudaMemcpyAsync(d->tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice,
+        SP_CUDA_TRY(cudaMemcpyAsync(d->tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice,
                                     ctx->stream));
     if (want_f32) {
         SP_CUDA_TRY(cudaMalloc(&d->v32, sizeof(float) * nz));

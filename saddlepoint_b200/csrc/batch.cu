@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -27,6 +28,13 @@ struct sp_batch {
     std::vector<void *> bufs;
     cudaGraphExec_t graph = nullptr;
     int grid = 0;
+    sp::BatchInst *d_inst = nullptr;
+    int *d_counter = nullptr;
+    double *av0 = nullptr, *tv0 = nullptr;  // the original values (the kernel scales in place)
+    size_t smem = 0;
+    double tuned_us[2][8] = {};  // per-iteration µs of each variant at the calibration sizes
+    int tuned_nnz[8] = {};
+    int tuned_points = 0;
 };
 
 namespace sp {
@@ -47,6 +55,140 @@ int balloc(sp_batch *b, T **p, int64_t n) {
     return SP_OK;
 }
 
+// The autotuner. Once per device it times the two SpMV variants — lane groups
+// (rows dealt to L lanes that walk them with strided loads) and staged tiles (the
+// single-LP tile passes) — on built-in seeded reference LPs that span the sizes of
+// the batched workload, each alone in one CTA, as the difference of a 320- and a
+// 64-iteration run (the scaling passes and the power iteration cancel). Every
+// instance then gets the variant whose interpolated per-iteration time at its size
+// (log nnz) is lower. The choice depends on the instance alone, never on the rest
+// of the batch, so an instance is computed the same way alone and in any mix.
+// SP_BATCH_VARIANT=lanes|tiles in the environment forces one variant.
+struct TuneTable {
+    bool ready = false;
+    int npts = 0;
+    int nnz[8] = {};
+    double us[2][8] = {};
+};
+static TuneTable g_tune[64];
+static std::mutex g_tune_mu;
+
+int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out,
+                 bool tune);
+
+int calibrate(sp_ctx *ctx, TuneTable *T) {
+    // reference LPs: the random LP recipe, m from 60 to 2000, n = 2m, 3-8 nonzeros per column
+    const int ms[] = {60, 180, 540, 2000};
+    std::vector<sp_lp> lps;
+    int rc = SP_OK;
+    for (int q = 0; q < 4 && !rc; ++q) {
+        sp_gen_params g{};
+        g.kind = SP_GEN_RANDOM;
+        g.seed = 0x5EED0000u + q;
+        g.nrows = ms[q];
+        g.ncols = 2 * ms[q];
+        g.nnz_per_col_min = 3;
+        g.nnz_per_col_max = 8;
+        sp_lp lp{};
+        rc = sp_generate(&g, &lp);
+        if (!rc) lps.push_back(lp);
+    }
+    sp_batch *b = nullptr;
+    if (!rc) rc = batch_create(ctx, lps.data(), (int)lps.size(), nullptr, &b, false);
+    if (!rc) {
+        cudaStream_t st = ctx->stream;
+        std::vector<BatchInst> &inst = b->inst;
+        int *d_one = nullptr;
+        rc = balloc(b, &d_one, 1);
+        BatchArgs A2 = b->args;
+        A2.count = 1;
+        A2.order = d_one;
+        A2.base.tolerance = 0.0;  // never converged: every run takes exactly its iterations
+        A2.power_iterations = std::min<unsigned long long>(A2.power_iterations, 4);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        auto run = [&](int c, unsigned long long iters, float *ms_out) -> int {
+            const BatchInst &I = inst[c];
+            A2.base.max_iterations = iters;
+            SP_CUDA_TRY(cudaMemcpyAsync(d_one, &c, sizeof(int), cudaMemcpyHostToDevice, st));
+            SP_CUDA_TRY(cudaMemcpyAsync(b->args.a_v + I.nz, b->av0 + I.nz, sizeof(double) * I.nnz,
+                                        cudaMemcpyDeviceToDevice, st));
+            SP_CUDA_TRY(cudaMemcpyAsync(b->args.t_v + I.nz, b->tv0 + I.nz, sizeof(double) * I.nnz,
+                                        cudaMemcpyDeviceToDevice, st));
+            SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+            SP_CUDA_TRY(cudaEventRecord(e0, st));
+            k_batch<NT><<<1, NT, b->smem, st>>>(A2);
+            SP_CUDA_TRY(cudaEventRecord(e1, st));
+            SP_CUDA_TRY(cudaEventSynchronize(e1));
+            SP_CUDA_TRY(cudaEventElapsedTime(ms_out, e0, e1));
+            return SP_OK;
+        };
+        const int npts = (int)inst.size();
+        for (int v = 0; v < 2 && !rc; ++v) {
+            for (auto &I : inst) I.variant = v;
+            rc = cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInst) * npts, cudaMemcpyHostToDevice) == cudaSuccess
+                     ? SP_OK
+                     : SP_ERR_CUDA;
+            for (int p = 0; p < npts && !rc; ++p) {
+                float t1 = 0, t2 = 0;
+                if ((rc = run(p, 64, &t1)) || (rc = run(p, 320, &t2))) break;
+                T->us[v][p] = std::max(0.0, (double)(t2 - t1) * 1e3 / 256.0);
+                T->nnz[p] = inst[p].nnz;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        T->npts = npts;
+        T->ready = rc == SP_OK;
+    }
+    if (b) sp_batch_free(b);
+    for (auto &lp : lps) sp_lp_release(&lp);
+    return rc;
+}
+
+int tune_variants(sp_batch *b) {
+    std::vector<BatchInst> &inst = b->inst;
+    int forced = -1;
+    if (const char *env = getenv("SP_BATCH_VARIANT"))
+        forced = !strcmp(env, "lanes") ? VARIANT_LANES : (!strcmp(env, "tiles") ? VARIANT_TILES : -1);
+    if (forced < 0) {
+        const int dev = b->ctx->device;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        if (dev < 0 || dev >= 64) return SP_ERR_INVALID;
+        if (!g_tune[dev].ready) {
+            int rc = calibrate(b->ctx, &g_tune[dev]);
+            if (rc) return rc;
+            set_current_ctx(b->ctx);
+        }
+        const TuneTable &T = g_tune[dev];
+        b->tuned_points = T.npts;
+        for (int p = 0; p < T.npts; ++p) {
+            b->tuned_nnz[p] = T.nnz[p];
+            b->tuned_us[0][p] = T.us[0][p];
+            b->tuned_us[1][p] = T.us[1][p];
+        }
+        auto estimate = [&](int v, int nnz) {
+            const double x = std::log(std::max(1, nnz));
+            if (T.npts == 1) return T.us[v][0];
+            int p = 0;
+            while (p + 2 < T.npts && std::log(std::max(1, T.nnz[p + 1])) < x) ++p;
+            const double x0 = std::log(std::max(1, T.nnz[p])), x1 = std::log(std::max(1, T.nnz[p + 1]));
+            const double f = x1 > x0 ? std::min(1.0, std::max(0.0, (x - x0) / (x1 - x0))) : 0.0;
+            return T.us[v][p] + f * (T.us[v][p + 1] - T.us[v][p]);
+        };
+        for (auto &I : inst)
+            I.variant =
+                estimate(VARIANT_TILES, I.nnz) <= estimate(VARIANT_LANES, I.nnz) ? VARIANT_TILES : VARIANT_LANES;
+    } else {
+        for (auto &I : inst) I.variant = forced;
+    }
+    cudaStream_t st = b->ctx->stream;
+    SP_CUDA_TRY(cudaMemcpyAsync(b->d_inst, inst.data(), sizeof(BatchInst) * b->count, cudaMemcpyHostToDevice, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
 }  // namespace sp
 
 using namespace sp;
@@ -62,6 +204,14 @@ extern "C" void sp_batch_free(sp_batch *b) {
 
 extern "C" int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params,
                                sp_batch **out) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    return batch_create(ctx, lps, count, params, out, true);
+}
+
+namespace sp {
+int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out,
+                 bool tune) {
     int rc = enter(ctx);
     if (rc) return rc;
     if (!lps || count <= 0 || !out) return fail(SP_ERR_INVALID, "sp_batch_create: bad arguments");
@@ -152,6 +302,44 @@ extern "C" int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const s
         for (int t = 0; t < nt; ++t) th.emplace_back(pack, count * t / nt, count * (t + 1) / nt);
         for (auto &t : th) t.join();
     }
+    // tile plans of every instance (tiles.cuh), for the tile variant
+    std::vector<std::vector<Tile>> tiles_a(count), tiles_t(count);
+    auto plan = [&](int i0, int i1) {
+        std::vector<int64_t> rp;
+        for (int i = i0; i < i1; ++i) {
+            const BatchInst &I = b->inst[i];
+            rp.assign(h_arp.begin() + I.rpa, h_arp.begin() + I.rpa + I.m + 1);
+            tiles_a[i] = build_tiles(rp.data(), I.m);
+            rp.assign(h_trp.begin() + I.rpt, h_trp.begin() + I.rpt + I.n + 1);
+            tiles_t[i] = build_tiles(rp.data(), I.n);
+        }
+    };
+    {
+        int nt = std::max(1, std::min<int>(16, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t) th.emplace_back(plan, count * t / nt, count * (t + 1) / nt);
+        for (auto &t : th) t.join();
+    }
+    int64_t n_ta = 0, n_tt = 0, n_part = 0;
+    for (int i = 0; i < count; ++i) {
+        BatchInst &I = b->inst[i];
+        I.ta = n_ta;
+        I.nta = (int)tiles_a[i].size();
+        n_ta += I.nta;
+        I.tt = n_tt;
+        I.ntt = (int)tiles_t[i].size();
+        n_tt += I.ntt;
+        I.pa = n_part;
+        n_part += (int64_t)I.nta * (NP_D + NP_D0);
+        I.pt = n_part;
+        n_part += (int64_t)I.ntt * (NP_P + NP_T + NP_P0 + 1);
+        I.variant = VARIANT_TILES;
+    }
+    std::vector<Tile> h_ta(std::max<int64_t>(n_ta, 1)), h_tt(std::max<int64_t>(n_tt, 1));
+    for (int i = 0; i < count; ++i) {
+        std::copy(tiles_a[i].begin(), tiles_a[i].end(), h_ta.begin() + b->inst[i].ta);
+        std::copy(tiles_t[i].begin(), tiles_t[i].end(), h_tt.begin() + b->inst[i].tt);
+    }
     // processing order: largest first, so the long instances start early
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
@@ -240,17 +428,31 @@ extern "C" int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const s
     A.pc_alpha = P.pock_chambolle_alpha;
     A.rescale = P.bound_objective_rescaling;
     A.step_size_factor = P.step_size_factor;
-    // one graph: restore the original values, reset the counter, run the persistent kernel
+    Tile *d_ta, *d_tt;
+    if ((rc = balloc(b, &d_ta, n_ta)) || (rc = balloc(b, &d_tt, n_tt)) || (rc = balloc(b, &A.part, n_part)) ||
+        (rc = up(d_ta, h_ta.data(), sizeof(Tile) * n_ta)) || (rc = up(d_tt, h_tt.data(), sizeof(Tile) * n_tt)))
+        return bail(rc, "sp_batch_create: tile plans");
+    A.a_tiles = d_ta;
+    A.t_tiles = d_tt;
+    const size_t smem = batch_smem_bytes();
+    SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_batch<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<NT>, NT, 0));
+    SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<NT>, NT, smem));
     b->grid = std::max(1, std::min(count, std::max(1, per_sm) * ctx->sms));
+    b->d_inst = d_inst;
+    b->d_counter = d_counter;
+    b->av0 = av0;
+    b->tv0 = tv0;
+    b->smem = smem;
+    if (tune && (rc = tune_variants(b))) return bail(rc, "sp_batch_create: tuner");
+    // one graph: restore the original values, reset the counter, run the persistent kernel
     cudaGraph_t g;
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(av, av0, sizeof(double) * nz, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(tv, tv0, sizeof(double) * nz, cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(d_counter, 0, sizeof(int), st);
-    k_batch<NT><<<b->grid, NT, 0, st>>>(A);
+    k_batch<NT><<<b->grid, NT, smem, st>>>(A);
     SP_CUDA_TRY(cudaStreamEndCapture(st, &g));
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
@@ -258,6 +460,8 @@ extern "C" int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const s
     *out = b;
     return SP_OK;
 }
+
+}  // namespace sp
 
 extern "C" int sp_batch_solve(sp_batch *b, sp_batch_result *results, double *elapsed_s) {
     if (!b) return SP_ERR_INVALID;

@@ -16,19 +16,25 @@
 #pragma once
 
 #include "control.cuh"
+#include "solver_kernels.cuh"
 
 namespace sp {
 
 struct BatchInst {
     int m, n, nnz;
-    int lanes_a, lanes_t;  // lanes per row for A' and for A'ᵀ
-    int pad;
+    int lanes_a, lanes_t;  // lanes per row for A' and for A'ᵀ (lane-group variant)
+    int variant;           // VARIANT_LANES or VARIANT_TILES, picked by the tuner
     long long rpa, rpt;    // offsets of the row pointers (m + 1 and n + 1 entries, instance-local values)
     long long nz;          // offset of the nonzeros
     long long mo, no;      // offsets of the m- and n-vectors
+    long long ta, tt;      // offsets of the tile plans of A' and A'ᵀ (instance-local rows)
+    long long pa, pt;      // offsets of the per-tile partial sums (10 per A' tile, 15 per A'ᵀ tile)
+    int nta, ntt;          // tiles of A' and A'ᵀ
     double c0;
     int maximize, pad2;
 };
+
+enum : int { VARIANT_LANES = 0, VARIANT_TILES = 1 };
 
 struct BatchArgs {
     const BatchInst *inst;
@@ -42,6 +48,8 @@ struct BatchArgs {
     double *c, *lc, *uc, *lv, *uv, *pf, *df, *rs, *cs;
     double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty, *pv, *pt, *ox, *oy;
     float *xbar32, *y32;
+    const Tile *a_tiles, *t_tiles;
+    double *part;  // per-tile partial sums of every instance
     sp_batch_result *res;
     DevParams base;
     unsigned long long power_iterations, geo_passes, ruiz_iterations;
@@ -90,8 +98,209 @@ struct Rows {
     }
 };
 
+// Runs a tile pass over one instance's tiles if its setup() accepts (uniform over the CTA).
+template <class Op>
+__device__ __forceinline__ void cta_tiles(Op op, int ntiles, unsigned char *dsm) {
+    if (!op.setup()) return;
+    for (int t = 0; t < ntiles; ++t) {
+        tile_body(op, dsm, t);
+        __syncthreads();
+    }
+}
+
+template <bool LO>
+__device__ __forceinline__ void cta_primal(const SolverPtrs &S, int role, int nt, unsigned char *dsm) {
+    auto mk = [&](auto tag) {
+        constexpr int MODE = decltype(tag)::value;
+        PrimalPass<LO, MODE> o{};
+        o.rp = S.t_rp;
+        o.ci = S.t_ci;
+        if constexpr (LO) o.vals = S.t_v32;
+        else o.vals = S.t_v;
+        o.tiles = S.t_tiles;
+        o.s = S;
+        o.i = 0;
+        o.role = role;
+        return o;
+    };
+    cta_tiles(mk(std::integral_constant<int, 0>{}), nt, dsm);
+    cta_tiles(mk(std::integral_constant<int, 1>{}), nt, dsm);
+    cta_tiles(mk(std::integral_constant<int, 2>{}), nt, dsm);
+}
+
+template <bool LO>
+__device__ __forceinline__ void cta_dual(const SolverPtrs &S, int role, int nt, unsigned char *dsm) {
+    auto mk = [&](auto tag) {
+        constexpr int MODE = decltype(tag)::value;
+        DualPass<LO, MODE> o{};
+        o.rp = S.a_rp;
+        o.ci = S.a_ci;
+        if constexpr (LO && MODE == 0) o.vals = S.a_v32;
+        else o.vals = S.a_v;
+        o.tiles = S.a_tiles;
+        o.s = S;
+        o.i = 0;
+        o.role = role;
+        return o;
+    };
+    cta_tiles(mk(std::integral_constant<int, 0>{}), nt, dsm);
+    cta_tiles(mk(std::integral_constant<int, 1>{}), nt, dsm);
+    cta_tiles(mk(std::integral_constant<int, 2>{}), nt, dsm);
+}
+
+// An instance solved by the tile passes of the single-LP solve, driven by this CTA
+// instead of by kernel launches: the same tiles, the same partial sums reduced in
+// the same order, the same controller — so the same bits as sp_solve.
 template <int BT>
-__device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState &st, DevParams &prm, double *bc) {
+__device__ void batch_tiles_solve(const BatchArgs &A, const BatchInst &I, const SolverPtrs &S, double *ppart,
+                                  double *pv, double *ptmp, double *sh, unsigned char *dsm, DevState &st,
+                                  DevParams &prm) {
+    static_assert(BT == NT, "the tile passes are written for NT threads");
+    const int tid = threadIdx.x, m = I.m, n = I.n;
+    const bool mixed = A.mixed != 0;
+    // power iteration (solver.rs:215-242), as k_power_init / PowerA / PowerT / k_power_fin
+    double lambda = 0.0;
+    bool numerical = false;
+    if (n > 0 && I.nnz > 0) {
+        double s1[1] = {0.0};
+        for (int j = tid; j < n; j += BT) {
+            const double v0 = 1.0 + 0.01 * (double)(j % 7);
+            pv[j] = v0;
+            s1[0] += v0 * v0;
+        }
+        block_sum<1>(s1, sh);
+        if (tid == 0) {
+            st.pi_scale = 1.0 / sqrt(s1[0]);
+            st.pi_lambda = 0.0;
+            st.pi_done = 0;
+            st.pi_iters = 0;
+            st.error = ERR_NONE;
+        }
+        __syncthreads();
+        for (unsigned long long it = 0; it < A.power_iterations && !st.pi_done; ++it) {
+            PowerA pa{S.a_rp, S.a_ci, S.a_v, S.a_tiles, pv, ptmp, &st, 0.0};
+            cta_tiles(pa, I.nta, dsm);
+            PowerT ptr{S.t_rp, S.t_ci, S.t_v, S.t_tiles, ptmp, pv, ppart, &st};
+            cta_tiles(ptr, I.ntt, dsm);
+            double s[1];
+            sum_slots<1>(ppart, I.ntt, s, sh);
+            if (tid == 0) {
+                const double norm = sqrt(s[0]);
+                if (isnan(norm) || norm <= 0.0 || isinf(norm)) {
+                    st.error = ERR_NUMERICAL_POWER;
+                    st.pi_done = 1;
+                } else {
+                    st.pi_scale = 1.0 / norm;
+                    const bool done = fabs(norm - st.pi_lambda) <= 1e-6 * norm;
+                    st.pi_lambda = norm;
+                    st.pi_iters += 1;
+                    if (done || (unsigned long long)st.pi_iters >= A.power_iterations) st.pi_done = 1;
+                }
+            }
+            __syncthreads();
+        }
+        lambda = st.pi_lambda;
+        numerical = st.error == ERR_NUMERICAL_POWER;
+    }
+    const double norm_est = (n > 0 && I.nnz > 0) ? sqrt(lambda) * 1.01 : 1.0;
+    __syncthreads();
+    if (tid == 0) {
+        prm.eta = A.step_size_factor / norm_est;
+        st = DevState{};
+        st.omega = A.rescale ? 1.0 : (1.0 + prm.c_norm) / (1.0 + prm.b_norm);
+        st.status = -1;
+        st.fp64 = mixed ? 0 : 1;
+        st.anchor_residual = INFINITY;
+        st.prev_residual = INFINITY;
+        st.pid_best_weight = st.omega;
+        st.pid_best_balance = INFINITY;
+        st.mx_best = INFINITY;
+        st.pi_done = 1;
+        if (numerical) {
+            st.done = 1;
+            st.error = ERR_NUMERICAL_POWER;
+        }
+    }
+    for (int j = tid; j < n; j += BT) S.x[j] = S.xa[j] = 0.0;
+    for (int i = tid; i < m; i += BT) {
+        S.y[i] = S.ya[i] = 0.0;
+        if (mixed) S.y32[i] = 0.0f;
+    }
+    __syncthreads();
+    // the PDHG loop (solver.rs:332-420), one iteration at a time
+    while (!st.done) {
+        const bool check = (prm.check_every != 0 && (st.total + 1) % prm.check_every == 0) ||
+                           st.total + 1 >= prm.max_iterations;
+        const bool k0 = st.k == 0;
+        const bool lo = mixed && !st.fp64;
+        const int role = check ? ROLE_CHECK : ROLE_FIRST;  // FIRST: K0 at k == 0, else fused
+        if (lo) cta_primal<true>(S, role, I.ntt, dsm);
+        else cta_primal<false>(S, role, I.ntt, dsm);
+        if (lo) cta_dual<true>(S, role, I.nta, dsm);
+        else cta_dual<false>(S, role, I.nta, dsm);
+        if (!check) {
+            if (k0) {
+                const double rho = prm.reflection;
+                for (int j = tid; j < n; j += BT) S.x[j] = halpern(S.x[j], S.xt[j], S.xa[j], 0.5, rho);
+                double P0[1], D0[2];
+                sum_slots<1>(S.partP0, I.ntt, P0, sh);
+                sum_slots<2>(S.partD0, I.nta, D0, sh);
+                if (tid == 0) {
+                    bool bad = false;
+                    st.anchor_residual = fixed_point_residual(prm.eta, st.omega, P0[0], D0[0], D0[1], &bad);
+                    if (bad) {
+                        st.error = ERR_NUMERICAL_ITERATES;
+                        st.done = 1;
+                    }
+                }
+            }
+            if (tid == 0) {
+                st.k += 1;
+                st.total += 1;
+            }
+            __syncthreads();
+            continue;
+        }
+        CheckPassT tp{};
+        tp.rp = S.t_rp;
+        tp.ci = S.t_ci;
+        tp.vals = S.t_v;
+        tp.tiles = S.t_tiles;
+        tp.s = S;
+        tp.i = 0;
+        cta_tiles(tp, I.ntt, dsm);
+        double P[NP_P], D[NP_D], T[NP_T];
+        sum_slots<NP_P>(S.partP, I.ntt, P, sh);
+        sum_slots<NP_D>(S.partD, I.nta, D, sh);
+        sum_slots<NP_T>(S.partT, I.ntt, T, sh);
+        if (tid == 0) {
+            bool bad = false;
+            sp_check_record rec;
+            check_decide(&st, &prm, P, D, T, st.k, st.total + 1, &bad, &rec);
+        }
+        __syncthreads();
+        if (st.done) break;
+        // k_finish: the Halpern step, or the restart's copies
+        const double w = st.w_last, rho = prm.reflection;
+        const bool rs = st.restart_flag != 0, y32 = mixed && !st.fp64;
+        for (int j = tid; j < n; j += BT) {
+            if (rs) S.x[j] = S.xa[j] = S.xt[j];
+            else S.x[j] = halpern(S.x[j], S.xt[j], S.xa[j], w, rho);
+        }
+        for (int i = tid; i < m; i += BT) {
+            double v;
+            if (rs) v = S.ya[i] = S.yt[i];
+            else v = halpern(S.y[i], S.yt[i], S.ya[i], w, rho);
+            S.y[i] = v;
+            if (y32) S.y32[i] = (float)v;
+        }
+        __syncthreads();
+    }
+}
+
+template <int BT>
+__device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState &st, DevParams &prm, double *bc,
+                                unsigned char *dsm) {
     const BatchInst I = A.inst[id];
     const int m = I.m, n = I.n;
     const int *arp = A.a_rp + I.rpa, *aci = A.a_ci + I.nz, *trp = A.t_rp + I.rpt, *tci = A.t_ci + I.nz;
@@ -242,6 +451,47 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
     }
     __syncthreads();
 
+    if (I.variant == VARIANT_TILES) {
+        SolverPtrs S{};
+        S.a_rp = arp;
+        S.a_ci = aci;
+        S.a_v = av;
+        S.a_v32 = av32;
+        S.a_tiles = A.a_tiles + I.ta;
+        S.t_rp = trp;
+        S.t_ci = tci;
+        S.t_v = tv;
+        S.t_v32 = tv32;
+        S.t_tiles = A.t_tiles + I.tt;
+        S.c = c;
+        S.lc = lc;
+        S.uc = uc;
+        S.lv = lv;
+        S.uv = uv;
+        S.pf = pf;
+        S.df = df;
+        S.x = x;
+        S.y = y;
+        S.xt = xt;
+        S.yt = A.yt + I.mo;
+        S.xbar = xbar;
+        S.xa = xa;
+        S.ya = ya;
+        S.aty = aty;
+        S.xbar32 = xbar32;
+        S.y32 = y32;
+        double *pt_base = A.part + I.pt, *pa_base = A.part + I.pa;
+        S.partP = pt_base;
+        S.partT = pt_base + (long long)I.ntt * NP_P;
+        S.partP0 = pt_base + (long long)I.ntt * (NP_P + NP_T);
+        S.partD = pa_base;
+        S.partD0 = pa_base + (long long)I.nta * NP_D;
+        S.prm = &prm;
+        S.st = &st;
+        S.mixed = mixed;
+        batch_tiles_solve<BT>(A, I, S, pt_base + (long long)I.ntt * (NP_P + NP_T + NP_P0), pv, pt, sh, dsm, st,
+                              prm);
+    } else {
     const Rows<BT> RA(I.lanes_a), RT(I.lanes_t);
 
     // ---------------- power iteration (solver.rs:215-242)
@@ -516,6 +766,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         }
         __syncthreads();
     }
+    }  // lane-group variant
     // Solution in the original space (solver.rs:422-437)
     for (int j = tid; j < n; j += BT) ox[j] = xt[j] * cs[j] / bs;
     for (int i = tid; i < m; i += BT) oy[i] = yt[i] * rs[i] / os;
@@ -530,7 +781,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         r.gap = fabs(st.primal_obj - st.dual_obj);
         r.iterations = st.total;
         r.restarts = st.restarts;
-        r.lanes_per_row = I.lanes_a * 100 + I.lanes_t;
+        r.lanes_per_row = I.variant == VARIANT_TILES ? 0 : I.lanes_a * 100 + I.lanes_t;
         A.res[id] = r;
     }
     __syncthreads();
@@ -538,6 +789,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
 
 template <int BT>
 __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
+    extern __shared__ __align__(16) unsigned char dsm[];  // tile staging of the tile variant
     __shared__ double sh[NP_P * (BT / 32)];
     __shared__ DevState st;
     __shared__ DevParams prm;
@@ -549,8 +801,11 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
         const int slot = next;
         __syncthreads();
         if (slot >= A.count) return;
-        batch_solve_one<BT>(A, A.order[slot], sh, st, prm, bc);
+        batch_solve_one<BT>(A, A.order[slot], sh, st, prm, bc, dsm);
     }
 }
+
+// Dynamic shared memory of k_batch: the largest tile pass (four products per nonzero).
+constexpr size_t batch_smem_bytes() { return tile_smem_bytes<4, double>(); }
 
 }  // namespace sp

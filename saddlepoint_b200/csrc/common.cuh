@@ -17,11 +17,14 @@
 namespace sp {
 
 constexpr int NT = 256;           // threads per CTA of every tile kernel
-constexpr int TILE_NNZ = 2048;    // nonzeros staged per tile
-constexpr int TILE_ROWS = 1024;   // rows per tile at most
+constexpr int TILE_NNZ = 2048;    // nonzeros staged per tile (8 per thread)
+constexpr int TILE_ROWS = 512;    // rows per tile at most
 constexpr int SEQ_MAX = 32;       // rows with at most this many entries are summed by one thread, in order
 constexpr int RED_BLOCKS = 592;   // 4 CTAs x 148 SMs: grid of the two-stage reductions
 constexpr int RED_SLOTS = 8;      // values one reduction call can produce
+
+// A row tile: {first row, end row, first nonzero, end nonzero}.
+using Tile = int4;
 
 // ---- the reference's scalar helpers (crates/saddlepoint-cpu/src/lib.rs:70-99, 262-269) ----
 

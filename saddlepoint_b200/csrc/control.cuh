@@ -22,6 +22,21 @@ constexpr int NP_D0 = 2;  // dual pass of a k == 0 iteration
 //   T[0] Σ(forbidden(c'-A'ᵀy_t)·f)²   T[1] Σ bound_term(c'-A'ᵀy_t)   T[2] step-implied dual residual²
 //   T[3] Σ forbidden(-A'ᵀ(y_t-y_a))²   T[4] Σ bound_term(-A'ᵀ(y_t-y_a))
 
+// Sums slot q of a [tiles x NPQ] partial array: each thread adds tiles t, t + NT, ...
+// in order, then a fixed tree over the block. The totals are valid in thread 0.
+template <int NPQ>
+__device__ void sum_slots(const double *part, int tiles, double (&out)[NPQ], double *sh) {
+    double v[NPQ];
+#pragma unroll
+    for (int q = 0; q < NPQ; ++q) v[q] = 0.0;
+    for (int t = threadIdx.x; t < tiles; t += NT)
+#pragma unroll
+        for (int q = 0; q < NPQ; ++q) v[q] += part[t * NPQ + q];
+    block_sum<NPQ>(v, sh);
+#pragma unroll
+    for (int q = 0; q < NPQ; ++q) out[q] = v[q];
+}
+
 // fixed_point_residual (solver.rs:275-288) from its three sums.
 __device__ __forceinline__ double fixed_point_residual(double eta, double omega, double dx2, double dy2, double cross,
                                                        bool *bad) {

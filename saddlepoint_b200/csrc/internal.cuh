@@ -34,7 +34,7 @@ struct DevCsr {
     int *ci = nullptr;
     double *v = nullptr;
     float *v32 = nullptr;
-    int2 *tiles = nullptr;
+    Tile *tiles = nullptr;
     int ntiles = 0;
 };
 

@@ -31,20 +31,6 @@ struct CtrlArgs {
     long long trace_cap;
 };
 
-// Sums slot q of a [tiles x NP] partial array in tile order per thread, then a fixed tree.
-template <int NPQ>
-__device__ void sum_slots(const double *part, int tiles, double (&out)[NPQ], double *sh) {
-    double v[NPQ];
-#pragma unroll
-    for (int q = 0; q < NPQ; ++q) v[q] = 0.0;
-    for (int t = threadIdx.x; t < tiles; t += NT)
-#pragma unroll
-        for (int q = 0; q < NPQ; ++q) v[q] += part[t * NPQ + q];
-    block_sum<NPQ>(v, sh);
-#pragma unroll
-    for (int q = 0; q < NPQ; ++q) out[q] = v[q];  // valid in thread 0
-}
-
 // The end of an epoch: the check iteration's decisions (solver.rs:339-419).
 __global__ void __launch_bounds__(NT) k_controller(CtrlArgs a, const DevParams *p, DevState *st) {
     __shared__ double sh[NP_P * (NT / 32)];
@@ -674,11 +660,11 @@ int transpose_on_device(sp_solver *s) {
     std::vector<int> rp32(n + 1);
     SP_CUDA_TRY(cudaMemcpy(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
     std::vector<int64_t> rp64(rp32.begin(), rp32.end());
-    std::vector<int2> tiles = build_tiles(rp64.data(), n);
+    std::vector<Tile> tiles = build_tiles(rp64.data(), n);
     T.ntiles = (int)tiles.size();
-    SP_CUDA_TRY(cudaMalloc(&T.tiles, sizeof(int2) * std::max<size_t>(tiles.size(), 1)));
+    SP_CUDA_TRY(cudaMalloc(&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
     if (!tiles.empty())
-        SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+        SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
     return SP_OK;
 }
 

@@ -31,7 +31,7 @@ struct SolverPtrs {
     const int *a_rp, *a_ci, *t_rp, *t_ci;
     const double *a_v, *t_v;
     const float *a_v32, *t_v32;
-    const int2 *a_tiles, *t_tiles;
+    const Tile *a_tiles, *t_tiles;
     // problem vectors
     const double *c, *lc, *uc, *lv, *uv, *pf, *df;
     // iterates
@@ -75,7 +75,7 @@ struct PrimalPass {
     static constexpr unsigned F32 = LO ? 1u : 0u;
     const int *rp, *ci;
     const VT *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     SolverPtrs s;
     int i, role;
     IterScalars sc;
@@ -91,24 +91,37 @@ struct PrimalPass {
         if constexpr (LO) p[0] = v * __ldg(s.y32 + c);
         else p[0] = v * __ldg(s.y + c);
     }
-    __device__ __forceinline__ void row(int j, const double (&sum)[1], double *part) const {
+    // The row's inputs, loaded at the start of the tile.
+    struct Pre {
+        double x, c, lv, uv, xa;
+    };
+    __device__ __forceinline__ Pre pre(int j) const {
+        Pre p;
+        p.x = __ldcs(s.x + j);
+        p.c = __ldcs(s.c + j);
+        p.lv = __ldcs(s.lv + j);
+        p.uv = __ldcs(s.uv + j);
+        p.xa = MODE == 1 ? 0.0 : __ldcs(s.xa + j);
+        return p;
+    }
+    __device__ __forceinline__ void row(int j, const double (&sum)[1], double *part, const Pre &in) const {
         const double aty = sum[0];
-        const double xj = s.x[j];
-        const double t = clampd(xj - sc.tau * (s.c[j] - aty), s.lv[j], s.uv[j]);  // cpu lib.rs:156
-        const double xb = 2.0 * t - xj;                                           // cpu lib.rs:158
+        const double xj = in.x;
+        const double t = clampd(xj - sc.tau * (in.c - aty), in.lv, in.uv);  // cpu lib.rs:156
+        const double xb = 2.0 * t - xj;                                     // cpu lib.rs:158
         if constexpr (LO) s.xbar32[j] = (float)xb;
         else s.xbar[j] = xb;
         if constexpr (MODE == 0) {
-            s.x[j] = halpern(xj, t, s.xa[j], sc.w, sc.rho);  // solver.rs:361
+            s.x[j] = halpern(xj, t, in.xa, sc.w, sc.rho);  // solver.rs:361
         } else {
             s.xt[j] = t;
             const double dx = t - xj;  // fixed_point_residual: x_t - x (solver.rs:277)
             part[0] += dx * dx;
             if constexpr (MODE == 2) {
                 s.aty[j] = aty;
-                const double cj = s.c[j];
-                const double dxa = t - s.xa[j];  // infeasibility: x_t - x_anchor (solver.rs:302)
-                const double rv = recession_violation(dxa, s.lv[j], s.uv[j]);
+                const double cj = in.c;
+                const double dxa = t - in.xa;  // infeasibility: x_t - x_anchor (solver.rs:302)
+                const double rv = recession_violation(dxa, in.lv, in.uv);
                 part[1] += cj * t;       // primal objective c'ᵀx_t
                 part[2] += aty * t;      // step-implied dual objective terms (solver.rs:268-269)
                 part[3] += t * t;
@@ -139,7 +152,7 @@ struct DualPass {
     static constexpr unsigned F32 = LO ? 1u : 0u;  // slot 0 is the iteration's product
     const int *rp, *ci;
     const VT *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     SolverPtrs s;
     int i, role;
     IterScalars sc;
@@ -163,12 +176,25 @@ struct DualPass {
             }
         }
     }
-    __device__ __forceinline__ void row(int r, const double (&sum)[G], double *part) const {
-        const double a = sum[0], yi = s.y[r];
-        const double v = a - yi / sc.sigma;                                  // cpu lib.rs:171
-        const double yt = yi - sc.sigma * (a - clampd(v, s.lc[r], s.uc[r])); // cpu lib.rs:172
+    // The row's inputs, loaded at the start of the tile.
+    struct Pre {
+        double y, lc, uc, ya, pf;
+    };
+    __device__ __forceinline__ Pre pre(int r) const {
+        Pre p;
+        p.y = __ldcs(s.y + r);
+        p.lc = __ldcs(s.lc + r);
+        p.uc = __ldcs(s.uc + r);
+        p.ya = __ldcs(s.ya + r);
+        p.pf = MODE == 2 ? __ldcs(s.pf + r) : 0.0;
+        return p;
+    }
+    __device__ __forceinline__ void row(int r, const double (&sum)[G], double *part, const Pre &in) const {
+        const double a = sum[0], yi = in.y;
+        const double v = a - yi / sc.sigma;                              // cpu lib.rs:171
+        const double yt = yi - sc.sigma * (a - clampd(v, in.lc, in.uc)); // cpu lib.rs:172
         if constexpr (MODE == 0) {
-            const double yn = halpern(yi, yt, s.ya[r], sc.w, sc.rho);
+            const double yn = halpern(yi, yt, in.ya, sc.w, sc.rho);
             s.y[r] = yn;
             if constexpr (LO) s.y32[r] = (float)yn;  // the FP32 shadow the next P pass gathers
         } else {
@@ -176,14 +202,14 @@ struct DualPass {
             part[0] += dy * dy;
             part[1] += dy * sum[1];     // cross term dyᵀ A'(x_t - x)
             if constexpr (MODE == 1) {
-                const double yn = halpern(yi, yt, s.ya[r], sc.w, sc.rho);
+                const double yn = halpern(yi, yt, in.ya, sc.w, sc.rho);
                 s.y[r] = yn;
                 if constexpr (LO) s.y32[r] = (float)yn;
             } else {
                 s.yt[r] = yt;
-                const double lc = s.lc[r], uc = s.uc[r];
-                const double e = excess(sum[2], lc, uc) * s.pf[r];
-                const double dya = yt - s.ya[r];
+                const double lc = in.lc, uc = in.uc;
+                const double e = excess(sum[2], lc, uc) * in.pf;
+                const double dya = yt - in.ya;
                 const double rv = recession_violation(sum[3], lc, uc);
                 const double fb = forbidden(dya, lc, uc);
                 part[2] += e * e;                       // primal residual
@@ -211,7 +237,7 @@ struct CheckPassT {
     static constexpr unsigned F32 = 0;
     const int *rp, *ci;
     const double *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     SolverPtrs s;
     int i;
     double inv_tau;
@@ -226,12 +252,19 @@ struct CheckPassT {
         p[0] = v * ytc;
         p[1] = v * (ytc - __ldg(s.ya + c));
     }
-    __device__ __forceinline__ void row(int j, const double (&sum)[2], double *part) const {
-        const double lv = s.lv[j], uv = s.uv[j], df = s.df[j];
+    struct Pre {
+        double lv, uv, df, c, aty, xt, x;
+    };
+    __device__ __forceinline__ Pre pre(int j) const {
+        return Pre{__ldcs(s.lv + j), __ldcs(s.uv + j), __ldcs(s.df + j), __ldcs(s.c + j),
+                   __ldcs(s.aty + j), __ldcs(s.xt + j), __ldcs(s.x + j)};
+    }
+    __device__ __forceinline__ void row(int j, const double (&sum)[2], double *part, const Pre &in) const {
+        const double lv = in.lv, uv = in.uv, df = in.df;
         const double aty_t = sum[0];
-        const double r = s.c[j] - aty_t;
+        const double r = in.c - aty_t;
         const double f = forbidden(r, lv, uv) * df;
-        const double sd = (s.aty[j] - aty_t - (s.xt[j] - s.x[j]) * inv_tau) * df;
+        const double sd = (in.aty - aty_t - (in.xt - in.x) * inv_tau) * df;
         const double ra = -sum[1];
         const double fa = forbidden(ra, lv, uv);
         part[0] += f * f;                   // dual residual
@@ -255,7 +288,7 @@ struct PowerA {  // tmp = A' (v * s)
     static constexpr unsigned F32 = 0;
     const int *rp, *ci;
     const double *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     const double *v;
     double *tmp;
     DevState *st;
@@ -265,10 +298,12 @@ struct PowerA {  // tmp = A' (v * s)
         scale = st->pi_scale;
         return true;
     }
+    struct Pre {};
+    __device__ __forceinline__ Pre pre(int) const { return {}; }
     __device__ __forceinline__ void prod(int c, double val, double (&p)[1]) const {
         p[0] = val * (__ldg(v + c) * scale);  // the gather sees v after `scale(v, s)`
     }
-    __device__ __forceinline__ void row(int r, const double (&s)[1], double *) const { tmp[r] = s[0]; }
+    __device__ __forceinline__ void row(int r, const double (&s)[1], double *, const Pre &) const { tmp[r] = s[0]; }
     __device__ void store(int, const double *) const {}
 };
 
@@ -279,14 +314,16 @@ struct PowerT {  // v = A'ᵀ tmp, partial ‖v‖²
     static constexpr unsigned F32 = 0;
     const int *rp, *ci;
     const double *vals;
-    const int2 *tiles;
+    const Tile *tiles;
     const double *tmp;
     double *v;
     double *part;
     DevState *st;
+    struct Pre {};
     __device__ bool setup() { return !st->pi_done; }
+    __device__ __forceinline__ Pre pre(int) const { return {}; }
     __device__ __forceinline__ void prod(int c, double val, double (&p)[1]) const { p[0] = val * __ldg(tmp + c); }
-    __device__ __forceinline__ void row(int r, const double (&s)[1], double *pp) const {
+    __device__ __forceinline__ void row(int r, const double (&s)[1], double *pp, const Pre &) const {
         v[r] = s[0];
         pp[0] += s[0] * s[0];
     }
@@ -296,7 +333,7 @@ struct PowerT {  // v = A'ᵀ tmp, partial ‖v‖²
 template <class Op>
 __device__ __forceinline__ bool try_run(Op &op, unsigned char *smem) {
     if (!op.setup()) return false;
-    tile_body(op, smem);
+    tile_body(op, smem, blockIdx.x);
     return true;
 }
 

@@ -3,15 +3,19 @@
 // A matrix is cut once, at load time, into tiles of consecutive rows holding at
 // most TILE_NNZ nonzeros and TILE_ROWS rows; a row longer than TILE_NNZ gets a
 // tile of its own. One CTA of NT threads processes one tile:
-//   1. stage: the tile's (col, value) pairs are read with coalesced loads, the
-//      gathered vector entries fetched, and the G products per nonzero written
-//      to shared memory;
-//   2. sum: a row of at most SEQ_MAX entries is summed by one thread in column
+//   1. load: every load of the tile is issued before any of them is used — the
+//      tile's row pointers, the inputs of the epilogue of this thread's first row
+//      (Op::pre), and the TILE_NNZ / NT (column, value) pairs of this thread — so a
+//      tile costs about two memory round trips (the pairs, then the gathers)
+//      instead of a chain of them;
+//   2. stage: the gathered vector entries are fetched and the G products per
+//      nonzero written to shared memory;
+//   3. sum: a row of at most SEQ_MAX entries is summed by one thread in column
 //      order (starting from -0.0 like Rust's `Iterator::sum`, so the FP64 result
 //      equals the reference CPU backend's bit for bit); a longer row is summed by
 //      one warp (lane-strided partial sums, then a fixed shuffle tree); a row of
 //      more than TILE_NNZ entries by the whole CTA (fixed tree);
-//   3. epilogue: Op::row() consumes the sums of each row (primal/dual step,
+//   4. epilogue: Op::row() consumes the sums of each row (primal/dual step,
 //      Halpern update, residual terms) and may accumulate NP partial sums, which
 //      the CTA reduces in a fixed order and writes to per-tile slots.
 // Everything is deterministic: the same inputs give the same bits on every run.
@@ -23,15 +27,20 @@
 
 namespace sp {
 
+constexpr int NNZ_PER_THREAD = TILE_NNZ / NT;
+constexpr int RP_PER_THREAD = (TILE_ROWS + 1 + NT - 1) / NT;
+static_assert(TILE_NNZ % NT == 0, "a tile is a whole number of slots per thread");
+
 // Host: cuts rows [0, nrows) into tiles. `rp` has nrows + 1 entries. Tiles that
 // hold a single row longer than TILE_NNZ come first so they start early.
-inline std::vector<int2> build_tiles(const int64_t *rp, int64_t nrows) {
-    std::vector<int2> longs, shorts;
+inline std::vector<Tile> build_tiles(const int64_t *rp, int64_t nrows) {
+    std::vector<Tile> longs, shorts;
+    auto tile = [&](int64_t a, int64_t b) { return make_int4((int)a, (int)b, (int)rp[a], (int)rp[b]); };
     int64_t r = 0;
     while (r < nrows) {
         int64_t len = rp[r + 1] - rp[r];
         if (len > TILE_NNZ) {
-            longs.push_back(make_int2((int)r, (int)(r + 1)));
+            longs.push_back(tile(r, r + 1));
             ++r;
             continue;
         }
@@ -42,7 +51,7 @@ inline std::vector<int2> build_tiles(const int64_t *rp, int64_t nrows) {
             nnz += l;
             ++r1;
         }
-        shorts.push_back(make_int2((int)r, (int)r1));
+        shorts.push_back(tile(r, r1));
         r = r1;
     }
     longs.insert(longs.end(), shorts.begin(), shorts.end());
@@ -70,10 +79,17 @@ __device__ __forceinline__ AT warp_row_sum(const ST *__restrict__ p, int a, int 
     return warp_sum_down(s);
 }
 
+// Streaming loads of the matrix: each element is read once per pass, so they are
+// hinted to leave L2 first, which keeps the gathered vectors resident there.
+__device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
+__device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
+
 template <class Op>
-__device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
+__device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile) {
     using VT = typename Op::VT;
     using ST = typename Op::ST;
+    using Pre = typename Op::Pre;
     constexpr int G = Op::G;
     constexpr int NP = Op::NP;
     constexpr unsigned F32 = Op::F32;  // bit q set: slot q accumulates in float
@@ -82,24 +98,26 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
     const int *__restrict__ rp = op.rp;
     const int *__restrict__ ci = op.ci;
     const VT *__restrict__ vals = op.vals;
+    const int tid = threadIdx.x;
 
-    const int2 t = op.tiles[blockIdx.x];
+    const Tile t = op.tiles[tile];
     const int r0 = t.x, nr = t.y - t.x;
-    const int k0 = rp[r0], nk = rp[t.y] - k0;
+    const int k0 = t.z, nk = t.w - t.z;
     double part[NP > 0 ? NP : 1];
 #pragma unroll
     for (int q = 0; q < (NP > 0 ? NP : 1); ++q) part[q] = 0.0;
 
     if (nk > TILE_NNZ) {
         // One long row: every thread sums a strided slice, then a fixed tree.
+        const Pre pre = op.pre(r0);
         float sf[G];
         double sd[G];
 #pragma unroll
         for (int q = 0; q < G; ++q) { sf[q] = -0.0f; sd[q] = -0.0; }
-        for (int e = threadIdx.x; e < nk; e += NT) {
+        for (int e = tid; e < nk; e += NT) {
             const int k = k0 + e;
             ST p[G];
-            op.prod(ci[k], vals[k], p);
+            op.prod(ld_stream(ci + k), ld_stream(vals + k), p);
 #pragma unroll
             for (int q = 0; q < G; ++q) {
                 if ((F32 >> q) & 1u) sf[q] += float(p[q]);
@@ -113,40 +131,65 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
             // A float slot is reduced in float through the same tree.
             if ((F32 >> q) & 1u) {
                 float s = warp_sum_down(sf[q]);
-                if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+                if ((tid & 31) == 0) sh[tid >> 5] = s;
                 __syncthreads();
-                if (threadIdx.x < 32) {
-                    float v = threadIdx.x < NT / 32 ? float(sh[threadIdx.x]) : 0.0f;
+                if (tid < 32) {
+                    float v = tid < NT / 32 ? float(sh[tid]) : 0.0f;
                     v = warp_sum_down(v);
                     tot[q] = v;
                 }
                 __syncthreads();
             } else {
                 double s = warp_sum_down(sd[q]);
-                if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+                if ((tid & 31) == 0) sh[tid >> 5] = s;
                 __syncthreads();
-                if (threadIdx.x < 32) {
-                    double v = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+                if (tid < 32) {
+                    double v = tid < NT / 32 ? sh[tid] : 0.0;
                     tot[q] = warp_sum_down(v);
                 }
                 __syncthreads();
             }
         }
-        if (threadIdx.x == 0) op.row(r0, tot, part);
+        if (tid == 0) op.row(r0, tot, part, pre);
     } else {
-        // Stage the products of the tile's nonzeros.
-#pragma unroll 4
-        for (int e = threadIdx.x; e < nk; e += NT) {
-            const int k = k0 + e;
-            ST p[G];
-            op.prod(ci[k], vals[k], p);
+        // 1. Issue every load before its first use.
+        int rpv[RP_PER_THREAD];
 #pragma unroll
-            for (int q = 0; q < G; ++q) prod[q * TILE_NNZ + e] = p[q];
+        for (int u = 0; u < RP_PER_THREAD; ++u) {
+            const int i = tid + u * NT;
+            rpv[u] = i <= nr ? rp[r0 + i] : 0;
         }
-        for (int i = threadIdx.x; i <= nr; i += NT) srp[i] = rp[r0 + i] - k0;
+        Pre pre{};
+        if (tid < nr) pre = op.pre(r0 + tid);
+        int cc[NNZ_PER_THREAD];
+        VT vv[NNZ_PER_THREAD];
+#pragma unroll
+        for (int u = 0; u < NNZ_PER_THREAD; ++u) {
+            const int e = tid + u * NT;
+            if (e < nk) {
+                cc[u] = ld_stream(ci + k0 + e);
+                vv[u] = ld_stream(vals + k0 + e);
+            }
+        }
+        // 2. Gathers and products into shared memory.
+#pragma unroll
+        for (int u = 0; u < NNZ_PER_THREAD; ++u) {
+            const int e = tid + u * NT;
+            if (e < nk) {
+                ST p[G];
+                op.prod(cc[u], vv[u], p);
+#pragma unroll
+                for (int q = 0; q < G; ++q) prod[q * TILE_NNZ + e] = p[q];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RP_PER_THREAD; ++u) {
+            const int i = tid + u * NT;
+            if (i <= nr) srp[i] = rpv[u] - k0;
+        }
         __syncthreads();
-        // Short rows: one thread per row, in column order.
-        for (int i = threadIdx.x; i < nr; i += NT) {
+        // 3–4. Short rows: one thread per row, in column order.
+        for (int i = tid; i < nr; i += NT) {
             const int a = srp[i], b = srp[i + 1];
             if (b - a <= SEQ_MAX) {
                 double s[G];
@@ -154,11 +197,12 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
                 for (int q = 0; q < G; ++q)
                     s[q] = ((F32 >> q) & 1u) ? double(seq_sum<float>(prod + q * TILE_NNZ, a, b))
                                              : seq_sum<double>(prod + q * TILE_NNZ, a, b);
-                op.row(r0 + i, s, part);
+                if (i == tid) op.row(r0 + i, s, part, pre);
+                else op.row(r0 + i, s, part, op.pre(r0 + i));
             }
         }
         // Longer rows: one warp per row.
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int warp = tid >> 5, lane = tid & 31;
         for (int i = warp; i < nr; i += NT / 32) {
             const int a = srp[i], b = srp[i + 1];
             if (b - a > SEQ_MAX) {
@@ -167,14 +211,14 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem) {
                 for (int q = 0; q < G; ++q)
                     s[q] = ((F32 >> q) & 1u) ? double(warp_row_sum<float>(prod + q * TILE_NNZ, a, b, lane))
                                              : warp_row_sum<double>(prod + q * TILE_NNZ, a, b, lane);
-                if (lane == 0) op.row(r0 + i, s, part);
+                if (lane == 0) op.row(r0 + i, s, part, op.pre(r0 + i));
             }
         }
     }
     if constexpr (NP > 0) {
         __syncthreads();
         block_sum<NP>(part, reinterpret_cast<double *>(smem));
-        if (threadIdx.x == 0) op.store(blockIdx.x, part);
+        if (tid == 0) op.store(tile, part);
     }
 }
 
@@ -184,21 +228,7 @@ template <class Op>
 __global__ void __launch_bounds__(NT) k_tiles(Op op) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (!op.setup()) return;
-    tile_body(op, smem);
-}
-
-// Mixed form: the same pass in two precisions, chosen per launch from the state
-// (FP32 SpMV until the switch to FP64, then FP64), so one graph serves both.
-template <class OpLo, class OpHi>
-__global__ void __launch_bounds__(NT) k_tiles2(OpLo lo, OpHi hi, const DevState *st) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    if (st->fp64) {
-        if (!hi.setup()) return;
-        tile_body(hi, smem);
-    } else {
-        if (!lo.setup()) return;
-        tile_body(lo, smem);
-    }
+    tile_body(op, smem, blockIdx.x);
 }
 
 }  // namespace sp

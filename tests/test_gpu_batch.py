@@ -66,6 +66,33 @@ def test_batch_instance_alone_equals_in_mix(batch_lps, gpu_backend):
         assert np.array_equal(xa, xm) and np.array_equal(ya, ym)
 
 
+@pytest.mark.parametrize("variant", ["tiles", "lanes"])
+def test_batch_variants_match_oracle(variant, batch_lps, gpu_backend, monkeypatch):
+    monkeypatch.setenv("SP_BATCH_VARIANT", variant)
+    b = sp().BatchSolver(batch_lps[:10], sp().SolverParams(tolerance=TOL), gpu_backend)
+    res, _ = b.solve()
+    for i, (lp, r) in enumerate(zip(batch_lps[:10], res)):
+        assert r.variant == variant
+        ref = oracle.solve(lp, tolerance=TOL)
+        assert sp().Status(r.status).name == ref.status
+        x, y = b.solution(i)
+        oracle.check(lp, x, y).verify(2 * TOL)
+
+
+def test_batch_tile_variant_equals_the_solo_device_solve(batch_lps, gpu_backend, monkeypatch):
+    """The tile variant drives the single-LP solve's own passes, tiles and reductions from
+    inside one CTA, so each instance's answer is the solo sp_solve's, bit for bit."""
+    monkeypatch.setenv("SP_BATCH_VARIANT", "tiles")
+    lps = batch_lps[:8] + [netlib_lp("afiro"), netlib_lp("adlittle")]
+    b = sp().BatchSolver(lps, sp().SolverParams(tolerance=TOL), gpu_backend)
+    res, _ = b.solve()
+    for i, lp in enumerate(lps):
+        solo = sp().solve(lp, sp().SolverParams(tolerance=TOL), gpu_backend)
+        x, y = b.solution(i)
+        assert res[i].iterations == solo.iterations, (i, res[i].iterations, solo.iterations)
+        assert np.array_equal(x, solo.x) and np.array_equal(y, solo.y), i
+
+
 def test_batch_repeat_is_identical(batch_lps, gpu_backend):
     b = sp().BatchSolver(batch_lps[:6], sp().SolverParams(tolerance=TOL), gpu_backend)
     r1, _ = b.solve()
