@@ -36,6 +36,7 @@ struct StoreOp {  // out = A x (Backend::spmv / spmv_t)
     const Tile *tiles;
     const double *x;
     double *out;
+    const uint16_t *sched;
     struct Pre {};
     __device__ bool setup() { return true; }
     __device__ __forceinline__ Pre pre(int) const { return {}; }
@@ -391,6 +392,11 @@ int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32) {
     if (!tiles.empty())
         SP_CUDA_TRY(cudaMemcpyAsync(d->tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice,
                                     ctx->stream));
+    const std::vector<uint16_t> sched = build_schedule(h->row_ptr, h->nrows, tiles);
+    SP_CUDA_TRY(cudaMalloc(&d->sched, sizeof(uint16_t) * std::max<int64_t>(h->nrows, 1)));
+    if (h->nrows)
+        SP_CUDA_TRY(cudaMemcpyAsync(d->sched, sched.data(), sizeof(uint16_t) * h->nrows, cudaMemcpyHostToDevice,
+                                    ctx->stream));
     if (want_f32) {
         SP_CUDA_TRY(cudaMalloc(&d->v32, sizeof(float) * nz));
     }
@@ -405,6 +411,7 @@ void free_csr(DevCsr *d) {
     cudaFree(d->v);
     cudaFree(d->v32);
     cudaFree(d->tiles);
+    cudaFree(d->sched);
     *d = DevCsr{};
 }
 
@@ -416,7 +423,7 @@ int upload_vec(sp_ctx *ctx, double **d, const double *h, int64_t n) {
 
 void launch_spmv(sp_ctx *ctx, const DevCsr &A, const double *x, double *out, cudaStream_t s) {
     if (A.ntiles == 0) return;
-    StoreOp op{A.rp, A.ci, A.v, A.tiles, x, out};
+    StoreOp op{A.rp, A.ci, A.v, A.tiles, x, out, A.sched};
     k_tiles<StoreOp><<<A.ntiles, NT, tile_smem_bytes<1, double>(), s>>>(op);
 }
 

@@ -36,6 +36,7 @@ struct DevCsr {
     float *v32 = nullptr;
     Tile *tiles = nullptr;
     int ntiles = 0;
+    uint16_t *sched = nullptr;  // row schedule of every tile (build_schedule)
 };
 
 int enter(sp_ctx *ctx);

@@ -361,6 +361,8 @@ SolverPtrs ptrs_of(sp_solver *s) {
     p.a_v = s->A.v;
     p.a_v32 = s->A.v32;
     p.a_tiles = s->A.tiles;
+    p.a_sched = s->A.sched;
+    p.t_sched = s->AT.sched;
     p.t_rp = s->AT.rp;
     p.t_ci = s->AT.ci;
     p.t_v = s->AT.v;
@@ -402,6 +404,7 @@ PrimalPass<LO, MODE> mkP(const SolverPtrs &p, int i, int role) {
     if constexpr (LO) o.vals = p.t_v32;
     else o.vals = p.t_v;
     o.tiles = p.t_tiles;
+    o.sched = p.t_sched;
     o.s = p;
     o.i = i;
     o.role = role;
@@ -415,6 +418,7 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
     if constexpr (LO && MODE == 0) o.vals = p.a_v32;
     else o.vals = p.a_v;
     o.tiles = p.a_tiles;
+    o.sched = p.a_sched;
     o.s = p;
     o.i = i;
     o.role = role;
@@ -473,6 +477,7 @@ void launch_T(sp_solver *s, int i, cudaStream_t st) {
     o.ci = p.t_ci;
     o.vals = p.t_v;
     o.tiles = p.t_tiles;
+    o.sched = p.t_sched;
     o.s = p;
     o.i = i;
     k_tiles_any<<<s->AT.ntiles, NT, smem_T(), st>>>(o);
@@ -665,6 +670,9 @@ int transpose_on_device(sp_solver *s) {
     SP_CUDA_TRY(cudaMalloc(&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
     if (!tiles.empty())
         SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+    const std::vector<uint16_t> sched = build_schedule(rp64.data(), n, tiles);
+    if ((rc = dalloc(&T.sched, n))) return rc;
+    if (n) SP_CUDA_TRY(cudaMemcpy(T.sched, sched.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
     return SP_OK;
 }
 

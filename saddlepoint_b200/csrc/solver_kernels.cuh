@@ -32,6 +32,7 @@ struct SolverPtrs {
     const double *a_v, *t_v;
     const float *a_v32, *t_v32;
     const Tile *a_tiles, *t_tiles;
+    const uint16_t *a_sched, *t_sched;
     // problem vectors
     const double *c, *lc, *uc, *lv, *uv, *pf, *df;
     // iterates
@@ -76,6 +77,7 @@ struct PrimalPass {
     const int *rp, *ci;
     const VT *vals;
     const Tile *tiles;
+    const uint16_t *sched;  // null: rows in order
     SolverPtrs s;
     int i, role;
     IterScalars sc;
@@ -153,6 +155,7 @@ struct DualPass {
     const int *rp, *ci;
     const VT *vals;
     const Tile *tiles;
+    const uint16_t *sched;  // null: rows in order
     SolverPtrs s;
     int i, role;
     IterScalars sc;
@@ -238,6 +241,7 @@ struct CheckPassT {
     const int *rp, *ci;
     const double *vals;
     const Tile *tiles;
+    const uint16_t *sched;  // null: rows in order
     SolverPtrs s;
     int i;
     double inv_tau;

@@ -21,6 +21,10 @@
 // Everything is deterministic: the same inputs give the same bits on every run.
 #pragma once
 
+#include <algorithm>
+#include <cstdint>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -56,6 +60,78 @@ inline std::vector<Tile> build_tiles(const int64_t *rp, int64_t nrows) {
     }
     longs.insert(longs.end(), shorts.begin(), shorts.end());
     return longs;
+}
+
+// Host: the order in which the threads of a tile take its rows (tile-local row
+// indices, one uint16 per row, stored at the tile's first row). Rows of at most
+// SEQ_MAX entries come first, longest first, dealt so that the 16 rows of every
+// half-warp start in 16 different 8-byte shared-memory banks as far as the rows
+// allow (the sequential sums then read shared memory without bank conflicts, and
+// the rows of a warp have similar lengths); rows summed by a warp come last,
+// flagged with SCHED_WARP, so that no warp has to search for them. The schedule
+// decides only which thread sums which row, never the order of a row's sum, so
+// the rows' results do not depend on it; passes that accumulate partial sums
+// across rows do not use it.
+constexpr int SCHED_WARP = 0x8000;
+
+inline std::vector<uint16_t> build_schedule(const int64_t *rp, int64_t nrows, const std::vector<Tile> &tiles) {
+    std::vector<uint16_t> sched((size_t)std::max<int64_t>(nrows, 0), 0);
+    std::vector<int> shortr, heavy, order;
+    std::vector<char> used;
+    for (const Tile &t : tiles) {
+        const int64_t r0 = t.x, nr = (int64_t)t.y - t.x, k0 = t.z;
+        if ((int64_t)t.w - t.z > TILE_NNZ) {  // one long row: the CTA-wide path
+            sched[r0] = SCHED_WARP;
+            continue;
+        }
+        shortr.clear();
+        heavy.clear();
+        for (int q = 0; q < nr; ++q) (rp[r0 + q + 1] - rp[r0 + q] > SEQ_MAX ? heavy : shortr).push_back(q);
+        std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
+            return rp[r0 + a + 1] - rp[r0 + a] > rp[r0 + b + 1] - rp[r0 + b];
+        });
+        order.clear();
+        used.assign(shortr.size(), 0);
+        size_t next = 0;
+        while (order.size() < shortr.size()) {
+            // one half-warp: distinct start banks among the next 64 candidates, then
+            // whatever comes next
+            unsigned mask = 0;
+            int placed = 0, seen = 0;
+            for (size_t c = next; c < shortr.size() && placed < 16 && seen < 64; ++c) {
+                if (used[c]) continue;
+                ++seen;
+                const int bank = (int)((rp[r0 + shortr[c]] - k0) & 15);
+                if (!((mask >> bank) & 1u)) {
+                    mask |= 1u << bank;
+                    used[c] = 1;
+                    order.push_back(shortr[c]);
+                    ++placed;
+                }
+            }
+            for (size_t c = next; c < shortr.size() && placed < 16; ++c)
+                if (!used[c]) {
+                    used[c] = 1;
+                    order.push_back(shortr[c]);
+                    ++placed;
+                }
+            while (next < shortr.size() && used[next]) ++next;
+        }
+        for (size_t i = 0; i < order.size(); ++i) sched[r0 + i] = (uint16_t)order[i];
+        for (size_t i = 0; i < heavy.size(); ++i) sched[r0 + order.size() + i] = (uint16_t)(heavy[i] | SCHED_WARP);
+    }
+    return sched;
+}
+
+// The row schedule of an op, if it carries one.
+template <class Op, class = void>
+struct has_sched : std::false_type {};
+template <class Op>
+struct has_sched<Op, std::void_t<decltype(std::declval<Op>().sched)>> : std::true_type {};
+template <class Op>
+__device__ __forceinline__ const uint16_t *sched_of(const Op &op) {
+    if constexpr (has_sched<Op>::value) return op.sched;
+    else return nullptr;
 }
 
 template <int G, class ST>
@@ -159,8 +235,12 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
             const int i = tid + u * NT;
             rpv[u] = i <= nr ? rp[r0 + i] : 0;
         }
+        // Passes that reduce partial sums keep the row order: the partials a thread
+        // accumulates depend on which rows it takes.
+        const uint16_t *sched = NP == 0 ? sched_of(op) : nullptr;
+        const int e0 = (sched && tid < nr) ? (int)__ldg(sched + r0 + tid) : tid;  // this thread's first slot
         Pre pre{};
-        if (tid < nr) pre = op.pre(r0 + tid);
+        if (tid < nr) pre = op.pre(r0 + (e0 & (SCHED_WARP - 1)));
         int cc[NNZ_PER_THREAD];
         VT vv[NNZ_PER_THREAD];
 #pragma unroll
@@ -188,31 +268,42 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
             if (i <= nr) srp[i] = rpv[u] - k0;
         }
         __syncthreads();
-        // 3–4. Short rows: one thread per row, in column order.
-        for (int i = tid; i < nr; i += NT) {
+        // 3–4. Short rows: one thread per row, in column order. Thread u takes slot
+        // u of the schedule (row u without one).
+        for (int u = tid; u < nr; u += NT) {
+            const int e = u == tid ? e0 : (sched ? (int)__ldg(sched + r0 + u) : u);
+            const int i = e & (SCHED_WARP - 1);
             const int a = srp[i], b = srp[i + 1];
-            if (b - a <= SEQ_MAX) {
+            if (sched ? !(e & SCHED_WARP) : b - a <= SEQ_MAX) {
                 double s[G];
 #pragma unroll
                 for (int q = 0; q < G; ++q)
                     s[q] = ((F32 >> q) & 1u) ? double(seq_sum<float>(prod + q * TILE_NNZ, a, b))
                                              : seq_sum<double>(prod + q * TILE_NNZ, a, b);
-                if (i == tid) op.row(r0 + i, s, part, pre);
+                if (u == tid) op.row(r0 + i, s, part, pre);
                 else op.row(r0 + i, s, part, op.pre(r0 + i));
             }
         }
-        // Longer rows: one warp per row.
+        // Longer rows: one warp per row (the flagged tail of the schedule).
         const int warp = tid >> 5, lane = tid & 31;
-        for (int i = warp; i < nr; i += NT / 32) {
+        auto warp_row = [&](int i) {
             const int a = srp[i], b = srp[i + 1];
-            if (b - a > SEQ_MAX) {
-                double s[G];
+            double s[G];
 #pragma unroll
-                for (int q = 0; q < G; ++q)
-                    s[q] = ((F32 >> q) & 1u) ? double(warp_row_sum<float>(prod + q * TILE_NNZ, a, b, lane))
-                                             : warp_row_sum<double>(prod + q * TILE_NNZ, a, b, lane);
-                if (lane == 0) op.row(r0 + i, s, part, op.pre(r0 + i));
+            for (int q = 0; q < G; ++q)
+                s[q] = ((F32 >> q) & 1u) ? double(warp_row_sum<float>(prod + q * TILE_NNZ, a, b, lane))
+                                         : warp_row_sum<double>(prod + q * TILE_NNZ, a, b, lane);
+            if (lane == 0) op.row(r0 + i, s, part, op.pre(r0 + i));
+        };
+        if (sched) {
+            for (int u = nr - 1 - warp; u >= 0; u -= NT / 32) {
+                const int e = __ldg(sched + r0 + u);
+                if (!(e & SCHED_WARP)) break;
+                warp_row(e & (SCHED_WARP - 1));
             }
+        } else {
+            for (int i = warp; i < nr; i += NT / 32)
+                if (srp[i + 1] - srp[i] > SEQ_MAX) warp_row(i);
         }
     }
     if constexpr (NP > 0) {
