@@ -303,7 +303,9 @@ def run_ours(args):
         cpu = cpu_baseline(lp, f64["scaled"], f64["norm_estimate"])
 
     clocks = f64["clocks"]
-    launches_per_epoch = 2 * ITERS_PER_STEP + 4
+    # per 64-iteration epoch: P and D of every iteration, the second (K0) P and D of the
+    # first, the Halpern x update of the first, the T pass, the controller, k_finish
+    launches_per_epoch = 2 * ITERS_PER_STEP + 6
     line = {
         "metric": "PDHG iter/s (FP64, device-resident)",
         "value": value,
@@ -435,9 +437,16 @@ def run_batch(args):
         t_max = dist.max(max(times))
         st = np.array([r.status for r in res])
         its = np.array([r.iterations for r in res])
+        handed = [r for r in res if r.handed_off]
+        # one persistent-kernel launch, plus the single-LP solves of the handed-off
+        # instances: 134 launches per 64-iteration epoch and about 700 for scaling,
+        # transpose and power iteration each
+        launches = 1 + sum(int(round(r.iterations / 64 * 134)) + 700 for r in handed)
         out[prec] = {"solves_per_s": dist.world * count / t_max, "s_per_batch": t_max,
                      "optimal": int((st == 0).sum()), "iterations_median": float(np.median(its)),
-                     "iterations_max": int(its.max()), "clocks": clk.summary()}
+                     "iterations_max": int(its.max()), "handed_off": len(handed),
+                     "handed_off_iterations": [int(r.iterations) for r in handed][:16],
+                     "gpu_launches_per_batch": launches, "clocks": clk.summary()}
         b.close()
     # the plain form: one device-resident solve per instance, on a spread sample
     sample = lps[:: count // 32]
@@ -471,7 +480,7 @@ def run_batch(args):
         "forms": {"fp64": f64, "mixed": out[sp.Precision.Mixed],
                   "plain_device_solve": {"solves_per_s": plain, "sample": len(sample), "optimal": plain_ok},
                   "batched_over_plain": f64["solves_per_s"] / plain},
-        "cpu_baseline": cpu, "gpu_launches": 1,
+        "cpu_baseline": cpu, "gpu_launches": f64["gpu_launches_per_batch"] * max(1, min(args.steps, 3)),
         "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     if dist.rank == 0:

@@ -90,6 +90,7 @@ class BatchResult(C.Structure):
     _fields_ = [
         ("status", cint), ("objective", dbl), ("dual_objective", dbl), ("primal_residual", dbl),
         ("dual_residual", dbl), ("gap", dbl), ("iterations", u64), ("restarts", u64), ("lanes_per_row", cint),
+        ("handed_off", cint),
     ]
 
 

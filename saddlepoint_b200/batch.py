@@ -39,6 +39,7 @@ class BatchResult:
     restarts: int
     lanes_a: int  # lanes per row the tuner picked for A' (0: the staged-tile variant)
     lanes_t: int  # ... and for A'ᵀ
+    handed_off: bool = False  # finished by the single-LP solver after outrunning its batch budget
 
     @property
     def variant(self) -> str:
@@ -76,7 +77,8 @@ class BatchSolver:
         t = C.c_double()
         self.backend._check(self.lib.sp_batch_solve(self.h, res, C.byref(t)))
         out = [BatchResult(r.status, r.objective, r.dual_objective, r.primal_residual, r.dual_residual, r.gap,
-                           int(r.iterations), int(r.restarts), r.lanes_per_row // 100, r.lanes_per_row % 100)
+                           int(r.iterations), int(r.restarts), r.lanes_per_row // 100, r.lanes_per_row % 100,
+                           bool(r.handed_off))
                for r in res]
         return out, t.value
 

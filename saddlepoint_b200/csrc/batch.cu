@@ -8,6 +8,7 @@
 // sp_batch_solve replays the graph; the scaling, power iteration and PDHG loop of
 // every instance run inside the kernel (batch_kernels.cuh).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -35,6 +36,7 @@ struct sp_batch {
     double tuned_us[2][8] = {};  // per-iteration µs of each variant at the calibration sizes
     int tuned_nnz[8] = {};
     int tuned_points = 0;
+    sp_solver_params params{};  // every instance's parameters (the hand-off solves use them too)
 };
 
 namespace sp {
@@ -75,6 +77,8 @@ static std::mutex g_tune_mu;
 
 int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out,
                  bool tune);
+
+constexpr double HANDOFF_MIN_US = 20.0;
 
 int calibrate(sp_ctx *ctx, TuneTable *T) {
     // reference LPs: the random LP recipe, m from 60 to 2000, n = 2m, 3-8 nonzeros per column
@@ -180,12 +184,154 @@ int tune_variants(sp_batch *b) {
         for (auto &I : inst)
             I.variant =
                 estimate(VARIANT_TILES, I.nnz) <= estimate(VARIANT_LANES, I.nnz) ? VARIANT_TILES : VARIANT_LANES;
+        // Hand-off budgets: an instance whose iterations would hold its CTA for more
+        // than SP_BATCH_HANDOFF_S seconds stops there (at a check iteration) and is
+        // solved again by the single-LP solver. Only instances slower per iteration
+        // inside the kernel than HANDOFF_MIN_US (SP_BATCH_HANDOFF_MIN_US) get one: for
+        // the others the single-LP solver, bound by its launch latency, would be no
+        // faster. A budget is a multiple of check_every and at least 16 of them.
+        double handoff_s = 4.0, min_us = HANDOFF_MIN_US;
+        if (const char *env = getenv("SP_BATCH_HANDOFF_S")) handoff_s = atof(env);
+        if (const char *env = getenv("SP_BATCH_HANDOFF_MIN_US")) min_us = atof(env);
+        const unsigned long long E = b->params.check_every ? b->params.check_every : 64;
+        for (auto &I : inst) {
+            I.budget = 0;
+            const double us = estimate(I.variant, I.nnz);
+            if (handoff_s > 0 && us > min_us) {
+                const unsigned long long it = (unsigned long long)(handoff_s * 1e6 / us);
+                I.budget = std::max<unsigned long long>(16 * E, it / E * E);
+            }
+        }
     } else {
         for (auto &I : inst) I.variant = forced;
     }
     cudaStream_t st = b->ctx->stream;
     SP_CUDA_TRY(cudaMemcpyAsync(b->d_inst, inst.data(), sizeof(BatchInst) * b->count, cudaMemcpyHostToDevice, st));
     SP_CUDA_TRY(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
+// The instance as an sp_lp again, from the arena's original data on the device.
+struct HostLp {
+    std::vector<int64_t> rp;
+    std::vector<int32_t> ci;
+    std::vector<double> v, c, lc, uc, lv, uv;
+    sp_lp lp{};
+};
+
+int download_instance(const sp_batch *b, int i, HostLp *h) {
+    const BatchInst &I = b->inst[i];
+    const BatchArgs &A = b->args;
+    std::vector<int> rp32(I.m + 1);
+    h->ci.resize(std::max(I.nnz, 1));
+    h->v.resize(std::max(I.nnz, 1));
+    h->c.resize(std::max(I.n, 1));
+    h->lv.resize(std::max(I.n, 1));
+    h->uv.resize(std::max(I.n, 1));
+    h->lc.resize(std::max(I.m, 1));
+    h->uc.resize(std::max(I.m, 1));
+    auto get = [](void *dst, const void *src, size_t bytes) -> int {
+        if (bytes) SP_CUDA_TRY(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return SP_OK;
+    };
+    int rc;
+    if ((rc = get(rp32.data(), A.a_rp + I.rpa, sizeof(int) * (I.m + 1))) ||
+        (rc = get(h->ci.data(), A.a_ci + I.nz, sizeof(int) * I.nnz)) ||
+        (rc = get(h->v.data(), b->av0 + I.nz, sizeof(double) * I.nnz)) ||
+        (rc = get(h->c.data(), A.oc + I.no, sizeof(double) * I.n)) ||
+        (rc = get(h->lv.data(), A.olv + I.no, sizeof(double) * I.n)) ||
+        (rc = get(h->uv.data(), A.ouv + I.no, sizeof(double) * I.n)) ||
+        (rc = get(h->lc.data(), A.olc + I.mo, sizeof(double) * I.m)) ||
+        (rc = get(h->uc.data(), A.ouc + I.mo, sizeof(double) * I.m)))
+        return rc;
+    h->rp.assign(rp32.begin(), rp32.end());
+    sp_lp &L = h->lp;
+    L.a.nrows = I.m;
+    L.a.ncols = I.n;
+    L.a.nnz = I.nnz;
+    L.a.row_ptr = h->rp.data();
+    L.a.col_idx = h->ci.data();
+    L.a.values = h->v.data();
+    L.c = h->c.data();
+    L.lc = h->lc.data();
+    L.uc = h->uc.data();
+    L.lv = h->lv.data();
+    L.uv = h->uv.data();
+    L.c0 = I.c0;
+    L.maximize = I.maximize;
+    return SP_OK;
+}
+
+// Solves the instances that stopped at their hand-off budget again with sp_solve,
+// up to eight at a time, each on a context (stream) of its own, and writes their
+// results and solutions where the kernel's would have gone.
+int hand_off(sp_batch *b, std::vector<sp_batch_result> &res) {
+    std::vector<int> todo;
+    for (int i = 0; i < b->count; ++i) {
+        const BatchInst &I = b->inst[i];
+        if (I.budget && I.budget < b->params.max_iterations && res[i].status == SP_STATUS_ITERATION_LIMIT &&
+            res[i].iterations >= I.budget)
+            todo.push_back(i);
+    }
+    if (todo.empty()) return SP_OK;
+    // the largest first, so the longest solves start early
+    std::stable_sort(todo.begin(), todo.end(), [&](int a, int c) { return b->inst[a].nnz > b->inst[c].nnz; });
+    const int workers = (int)std::min<size_t>(8, todo.size());
+    std::atomic<size_t> next{0};
+    std::mutex mu;
+    int first_err = SP_OK;
+    std::string err_msg;
+    auto work = [&]() {
+        sp_ctx *ctx = nullptr;
+        int rc = sp_ctx_create(b->ctx->device, &ctx);
+        size_t k;
+        while (!rc && (k = next.fetch_add(1)) < todo.size()) {
+            const int i = todo[k];
+            const BatchInst &I = b->inst[i];
+            HostLp h;
+            std::vector<double> x(std::max(I.n, 1)), y(std::max(I.m, 1));
+            sp_solution_info info{};
+            if ((rc = download_instance(b, i, &h))) break;
+            sp_batch_result &r = res[i];
+            rc = sp_solve(ctx, &h.lp, &b->params, x.data(), y.data(), &info);
+            if (rc == SP_ERR_NUMERICAL) {
+                // a breakdown is this instance's result, as the kernel reports it
+                const bool power = ctx->last_error.find("power") != std::string::npos;
+                r.status = -1 - (power ? ERR_NUMERICAL_POWER : ERR_NUMERICAL_ITERATES);
+                r.handed_off = 1;
+                rc = SP_OK;
+                continue;
+            }
+            if (rc) break;
+            if (I.n && cudaMemcpy(b->args.ox + I.no, x.data(), sizeof(double) * I.n, cudaMemcpyHostToDevice))
+                rc = SP_ERR_CUDA;
+            if (I.m && cudaMemcpy(b->args.oy + I.mo, y.data(), sizeof(double) * I.m, cudaMemcpyHostToDevice))
+                rc = SP_ERR_CUDA;
+            r.status = info.status;
+            r.objective = info.objective;
+            r.dual_objective = info.dual_objective;
+            r.primal_residual = info.primal_residual;
+            r.dual_residual = info.dual_residual;
+            r.gap = info.gap;
+            r.iterations = info.iterations;
+            r.restarts = info.restarts;
+            r.handed_off = 1;
+        }
+        if (rc) {
+            std::lock_guard<std::mutex> lock(mu);
+            if (!first_err) {
+                first_err = rc;
+                err_msg = ctx ? ctx->last_error : std::string("sp_ctx_create failed");
+            }
+        }
+        if (ctx) sp_ctx_destroy(ctx);
+    };
+    std::vector<std::thread> th;
+    for (int w = 0; w < workers; ++w) th.emplace_back(work);
+    for (auto &t : th) t.join();
+    set_current_ctx(b->ctx);
+    SP_CUDA_TRY(cudaSetDevice(b->ctx->device));
+    if (first_err) return fail(first_err, "batch hand-off solve: " + err_msg);
     return SP_OK;
 }
 
@@ -221,6 +367,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
     auto *b = new sp_batch();
     b->ctx = ctx;
     b->count = count;
+    b->params = P;
     b->mixed = P.precision == SP_PRECISION_MIXED;
     auto bail = [&](int code, const std::string &msg) {
         sp_batch_free(b);
@@ -395,6 +542,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
         if ((rc = balloc(b, p, no))) return bail(rc, "out of device memory");
     for (double **p : mvecs)
         if ((rc = balloc(b, p, mo))) return bail(rc, "out of device memory");
+    if ((rc = balloc(b, &A.pk, no))) return bail(rc, "out of device memory");
     A.a_v32 = A.t_v32 = nullptr;
     A.xbar32 = A.y32 = nullptr;
     if (b->mixed) {
@@ -479,9 +627,13 @@ extern "C" int sp_batch_solve(sp_batch *b, sp_batch_result *results, double *ela
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (elapsed_s) *elapsed_s = ms * 1e-3;
-    if (results)
-        SP_CUDA_TRY(cudaMemcpy(results, b->args.res, sizeof(sp_batch_result) * b->count, cudaMemcpyDeviceToHost));
+    std::vector<sp_batch_result> res(b->count);
+    SP_CUDA_TRY(cudaMemcpy(res.data(), b->args.res, sizeof(sp_batch_result) * b->count, cudaMemcpyDeviceToHost));
+    const auto t0 = std::chrono::steady_clock::now();
+    if ((rc = hand_off(b, res))) return rc;
+    const double handoff_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (elapsed_s) *elapsed_s = ms * 1e-3 + handoff_s;
+    if (results) std::copy(res.begin(), res.end(), results);
     return SP_OK;
 }
 

@@ -32,6 +32,7 @@ struct BatchInst {
     int nta, ntt;          // tiles of A' and A'ᵀ
     double c0;
     int maximize, pad2;
+    unsigned long long budget;  // iteration cap inside the batch (0: the solve's own limit)
 };
 
 enum : int { VARIANT_LANES = 0, VARIANT_TILES = 1 };
@@ -48,6 +49,7 @@ struct BatchArgs {
     double *c, *lc, *uc, *lv, *uv, *pf, *df, *rs, *cs;
     double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty, *pv, *pt, *ox, *oy;
     float *xbar32, *y32;
+    CheckQuad *pk;  // the tile variant's packed column records (n per instance)
     const Tile *a_tiles, *t_tiles;
     double *part;  // per-tile partial sums of every instance
     sp_batch_result *res;
@@ -423,6 +425,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         bc[0] = bs;
         bc[1] = os;
         prm = A.base;
+        if (I.budget && I.budget < prm.max_iterations) prm.max_iterations = I.budget;
         prm.b_norm = fbn(olc, ouc);
         prm.c_norm = n2(oc);
         prm.c0 = I.c0;
@@ -480,6 +483,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         S.aty = aty;
         S.xbar32 = xbar32;
         S.y32 = y32;
+        S.pk = A.pk + I.no;
         double *pt_base = A.part + I.pt, *pa_base = A.part + I.pa;
         S.partP = pt_base;
         S.partT = pt_base + (long long)I.ntt * NP_P;
@@ -782,6 +786,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         r.iterations = st.total;
         r.restarts = st.restarts;
         r.lanes_per_row = I.variant == VARIANT_TILES ? 0 : I.lanes_a * 100 + I.lanes_t;
+        r.handed_off = 0;
         A.res[id] = r;
     }
     __syncthreads();

@@ -385,6 +385,7 @@ SolverPtrs ptrs_of(sp_solver *s) {
     p.aty = s->aty;
     p.xbar32 = s->xbar32;
     p.y32 = s->y32;
+    p.pk = s->pk;
     p.partP = s->partP;
     p.partD = s->partD;
     p.partT = s->partT;
@@ -434,15 +435,20 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     if (s->mixed) {
         if (role == ROLE_MID)
             k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
-        else if (role == ROLE_FIRST)
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<true, 1>(p, i, role), mkP<false, 0>(p, i, role),
-                                           mkP<false, 1>(p, i, role));
+        else if (role == ROLE_FIRST) {
+            // FUSED and K0 as launches of their own (one of them returns at once), so
+            // the FUSED one keeps its own register and shared-memory footprint
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 1>(p, i, role), mkP<false, 1>(p, i, role));
+        }
         else
             k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 2>(p, i, role), mkP<false, 2>(p, i, role));
     } else {
         if (role == ROLE_MID) k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
-        else if (role == ROLE_FIRST)
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role), mkP<false, 1>(p, i, role));
+        else if (role == ROLE_FIRST) {
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
+            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 1>(p, i, role));
+        }
         else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 2>(p, i, role));
     }
 }
@@ -455,16 +461,19 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
     if (s->mixed) {
         if (role == ROLE_MID)
             k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
-        else if (role == ROLE_FIRST)
-            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<true, 1>(p, i, role),
-                                                                     mkD<false, 0>(p, i, role), mkD<false, 1>(p, i, role));
+        else if (role == ROLE_FIRST) {
+            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
+            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<true, 1>(p, i, role), mkD<false, 1>(p, i, role));
+        }
         else
             k_tiles_any<<<g, NT, sm, st>>>(mkD<true, 2>(p, i, role), mkD<false, 2>(p, i, role));
     } else {
         if (role == ROLE_MID)
             k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<false, 0>(p, i, role));
-        else if (role == ROLE_FIRST)
-            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<false, 0>(p, i, role), mkD<false, 1>(p, i, role));
+        else if (role == ROLE_FIRST) {
+            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<false, 0>(p, i, role));
+            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<false, 1>(p, i, role));
+        }
         else k_tiles_any<<<g, NT, sm, st>>>(mkD<false, 2>(p, i, role));
     }
 }
@@ -559,7 +568,7 @@ void solver_release(sp_solver *s) {
     free_csr(&s->A);
     free_csr(&s->AT);
     void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
-                    s->aty, s->xbar32, s->y32, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
+                    s->aty, s->xbar32, s->y32, s->pk, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
                     s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,
                     s->out_x, s->out_y};
     for (void *b : bufs) cudaFree(b);
@@ -835,6 +844,7 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     if ((rc = dalloc(&s->x, n)) || (rc = dalloc(&s->y, m)) || (rc = dalloc(&s->xt, n)) || (rc = dalloc(&s->yt, m)) ||
         (rc = dalloc(&s->xbar, n)) || (rc = dalloc(&s->xa, n)) || (rc = dalloc(&s->ya, m)) ||
         (rc = dalloc(&s->aty, n)) || (rc = dalloc(&s->xbar32, n)) || (rc = dalloc(&s->y32, m)) ||
+        (rc = dalloc(&s->pk, n)) ||
         (rc = dalloc(&s->partP, (int64_t)s->AT.ntiles * NP_P)) || (rc = dalloc(&s->partT, (int64_t)s->AT.ntiles * NP_T)) ||
         (rc = dalloc(&s->partP0, (int64_t)s->AT.ntiles * NP_P0)) ||
         (rc = dalloc(&s->partD, (int64_t)s->A.ntiles * NP_D)) || (rc = dalloc(&s->partD0, (int64_t)s->A.ntiles * NP_D0)) ||

@@ -25,6 +25,14 @@ namespace sp {
 
 enum Role : int { ROLE_FIRST = 0, ROLE_MID = 1, ROLE_CHECK = 2 };
 
+// What the dual pass of a check (and of the first iteration at k = 0) gathers per
+// column, packed into one 32-byte sector: x̄ (in the iteration precision), x_t - x,
+// x_t and x_t - x_anchor, each rounded exactly as the vector the reference forms
+// before its SpMV. Written by the primal pass of the same iteration.
+struct __align__(32) CheckQuad {
+    double xbar, dx, xt, dxa;
+};
+
 // Pointers of the device-resident solve.
 struct SolverPtrs {
     // A' (rows i) and A'ᵀ (rows j)
@@ -38,6 +46,7 @@ struct SolverPtrs {
     // iterates
     double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty;
     float *xbar32, *y32;
+    CheckQuad *pk;
     // partial sums per tile
     double *partP, *partD, *partT, *partP0, *partD0;
     const DevParams *prm;
@@ -119,10 +128,13 @@ struct PrimalPass {
             s.xt[j] = t;
             const double dx = t - xj;  // fixed_point_residual: x_t - x (solver.rs:277)
             part[0] += dx * dx;
+            const double xbq = LO ? (double)(float)xb : xb;  // x̄ as the dual pass gathers it
+            if constexpr (MODE == 1) s.pk[j] = CheckQuad{xbq, dx, t, 0.0};
             if constexpr (MODE == 2) {
                 s.aty[j] = aty;
                 const double cj = in.c;
                 const double dxa = t - in.xa;  // infeasibility: x_t - x_anchor (solver.rs:302)
+                s.pk[j] = CheckQuad{xbq, dx, t, dxa};
                 const double rv = recession_violation(dxa, in.lv, in.uv);
                 part[1] += cj * t;       // primal objective c'ᵀx_t
                 part[2] += aty * t;      // step-implied dual objective terms (solver.rs:268-269)
@@ -168,14 +180,20 @@ struct DualPass {
         return true;
     }
     __device__ __forceinline__ void prod(int c, VT v, ST (&p)[G]) const {
-        if constexpr (LO) p[0] = ST((float)v * __ldg(s.xbar32 + c));
-        else p[0] = v * __ldg(s.xbar + c);
-        if constexpr (MODE >= 1) {
-            const double xtc = __ldg(s.xt + c);
-            p[1] = v * (xtc - __ldg(s.x + c));  // A'(x_t - x)
+        if constexpr (MODE == 0) {
+            if constexpr (LO) p[0] = ST((float)v * __ldg(s.xbar32 + c));
+            else p[0] = v * __ldg(s.xbar + c);
+        } else {
+            // one sector per nonzero: the packed column record of the primal pass
+            const double2 *q = reinterpret_cast<const double2 *>(s.pk + c);
+            const double2 q0 = __ldg(q);
+            if constexpr (LO) p[0] = ST((float)v * (float)q0.x);
+            else p[0] = v * q0.x;
+            p[1] = v * q0.y;  // A'(x_t - x)
             if constexpr (MODE == 2) {
-                p[2] = v * xtc;                      // A' x_t
-                p[3] = v * (xtc - __ldg(s.xa + c));  // A'(x_t - x_anchor)
+                const double2 q1 = __ldg(q + 1);
+                p[2] = v * q1.x;  // A' x_t
+                p[3] = v * q1.y;  // A'(x_t - x_anchor)
             }
         }
     }

@@ -31,6 +31,7 @@ struct sp_solver {
     double *x = nullptr, *y = nullptr, *xt = nullptr, *yt = nullptr, *xbar = nullptr, *xa = nullptr, *ya = nullptr,
            *aty = nullptr;
     float *xbar32 = nullptr, *y32 = nullptr;
+    sp::CheckQuad *pk = nullptr;  // the check's packed column records
     // partial sums per tile
     double *partP = nullptr, *partD = nullptr, *partT = nullptr, *partP0 = nullptr, *partD0 = nullptr;
     // power iteration

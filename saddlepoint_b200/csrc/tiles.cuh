@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <thread>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -76,49 +77,64 @@ constexpr int SCHED_WARP = 0x8000;
 
 inline std::vector<uint16_t> build_schedule(const int64_t *rp, int64_t nrows, const std::vector<Tile> &tiles) {
     std::vector<uint16_t> sched((size_t)std::max<int64_t>(nrows, 0), 0);
-    std::vector<int> shortr, heavy, order;
-    std::vector<char> used;
-    for (const Tile &t : tiles) {
-        const int64_t r0 = t.x, nr = (int64_t)t.y - t.x, k0 = t.z;
-        if ((int64_t)t.w - t.z > TILE_NNZ) {  // one long row: the CTA-wide path
-            sched[r0] = SCHED_WARP;
-            continue;
-        }
-        shortr.clear();
-        heavy.clear();
-        for (int q = 0; q < nr; ++q) (rp[r0 + q + 1] - rp[r0 + q] > SEQ_MAX ? heavy : shortr).push_back(q);
-        std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
-            return rp[r0 + a + 1] - rp[r0 + a] > rp[r0 + b + 1] - rp[r0 + b];
-        });
-        order.clear();
-        used.assign(shortr.size(), 0);
-        size_t next = 0;
-        while (order.size() < shortr.size()) {
-            // one half-warp: distinct start banks among the next 64 candidates, then
-            // whatever comes next
-            unsigned mask = 0;
-            int placed = 0, seen = 0;
-            for (size_t c = next; c < shortr.size() && placed < 16 && seen < 64; ++c) {
-                if (used[c]) continue;
-                ++seen;
-                const int bank = (int)((rp[r0 + shortr[c]] - k0) & 15);
-                if (!((mask >> bank) & 1u)) {
-                    mask |= 1u << bank;
-                    used[c] = 1;
-                    order.push_back(shortr[c]);
-                    ++placed;
-                }
+    // tiles own disjoint rows: blocks of tiles go to host threads
+    auto run = [&](size_t t0, size_t t1) {
+        std::vector<int> shortr, heavy, order;
+        std::vector<char> used;
+        for (size_t ti = t0; ti < t1; ++ti) {
+            const Tile &t = tiles[ti];
+            const int64_t r0 = t.x, nr = (int64_t)t.y - t.x, k0 = t.z;
+            if ((int64_t)t.w - t.z > TILE_NNZ) {  // one long row: the CTA-wide path
+                sched[r0] = SCHED_WARP;
+                continue;
             }
-            for (size_t c = next; c < shortr.size() && placed < 16; ++c)
-                if (!used[c]) {
-                    used[c] = 1;
-                    order.push_back(shortr[c]);
-                    ++placed;
+            shortr.clear();
+            heavy.clear();
+            for (int q = 0; q < nr; ++q) (rp[r0 + q + 1] - rp[r0 + q] > SEQ_MAX ? heavy : shortr).push_back(q);
+            std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
+                return rp[r0 + a + 1] - rp[r0 + a] > rp[r0 + b + 1] - rp[r0 + b];
+            });
+            order.clear();
+            used.assign(shortr.size(), 0);
+            size_t next = 0;
+            while (order.size() < shortr.size()) {
+                // one half-warp: distinct start banks among the next 64 candidates, then
+                // whatever comes next
+                unsigned mask = 0;
+                int placed = 0, seen = 0;
+                for (size_t c = next; c < shortr.size() && placed < 16 && seen < 64; ++c) {
+                    if (used[c]) continue;
+                    ++seen;
+                    const int bank = (int)((rp[r0 + shortr[c]] - k0) & 15);
+                    if (!((mask >> bank) & 1u)) {
+                        mask |= 1u << bank;
+                        used[c] = 1;
+                        order.push_back(shortr[c]);
+                        ++placed;
+                    }
                 }
-            while (next < shortr.size() && used[next]) ++next;
+                for (size_t c = next; c < shortr.size() && placed < 16; ++c)
+                    if (!used[c]) {
+                        used[c] = 1;
+                        order.push_back(shortr[c]);
+                        ++placed;
+                    }
+                while (next < shortr.size() && used[next]) ++next;
+            }
+            for (size_t i = 0; i < order.size(); ++i) sched[r0 + i] = (uint16_t)order[i];
+            for (size_t i = 0; i < heavy.size(); ++i)
+                sched[r0 + order.size() + i] = (uint16_t)(heavy[i] | SCHED_WARP);
         }
-        for (size_t i = 0; i < order.size(); ++i) sched[r0 + i] = (uint16_t)order[i];
-        for (size_t i = 0; i < heavy.size(); ++i) sched[r0 + order.size() + i] = (uint16_t)(heavy[i] | SCHED_WARP);
+    };
+    const size_t nt = tiles.size();
+    const int workers = (int)std::min<size_t>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())),
+                                              std::max<size_t>(1, nt / 256));
+    if (workers <= 1) {
+        run(0, nt);
+    } else {
+        std::vector<std::thread> th;
+        for (int w = 0; w < workers; ++w) th.emplace_back(run, nt * w / workers, nt * (w + 1) / workers);
+        for (auto &t : th) t.join();
     }
     return sched;
 }
