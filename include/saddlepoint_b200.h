@@ -243,18 +243,19 @@ typedef struct {
     uint64_t iterations, restarts;
     int lanes_per_row; /* SpMV variant the tuner chose: 0 = staged tiles (the single-LP passes);
                           otherwise lane groups, 100 * (lanes per row of A') + (lanes per row of A'ᵀ) */
-    int handed_off;    /* 1: the instance outran its share of the persistent kernel and was solved
-                          again from the start by the single-LP device solver (sp_solve) */
+    int handed_off;    /* 1: the instance was still running well after every other instance had
+                          been started, and was solved again from the start by the single-LP
+                          device solver (sp_solve) */
 } sp_batch_result;
 
 /* Scales and uploads `count` LPs into one packed arena. */
 int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out);
-/* Solves every instance; results[count]. An instance whose iterations inside the
- * persistent kernel would occupy its CTA for more than SP_BATCH_HANDOFF_S seconds
- * (environment, default 4; 0 turns this off), as the tuner's per-iteration
- * timings predict, is stopped there and solved again from the start by the
- * single-LP device solver, several such instances at once on their own streams;
- * its result is then exactly sp_solve's. *elapsed_s covers both. */
+/* Solves every instance; results[count]. An instance still running in the
+ * persistent kernel SP_BATCH_HANDOFF_S seconds (environment, default 2; 0 turns
+ * this off) after the last instance was started stops at its next check and is
+ * solved again from the start by the single-LP device solver, several such
+ * instances at once on their own streams; its result is then exactly sp_solve's.
+ * *elapsed_s covers both. */
 int sp_batch_solve(sp_batch *b, sp_batch_result *results, double *elapsed_s);
 /* x/y of instance i in the original space. */
 int sp_batch_download(sp_batch *b, int i, double *x, double *y);

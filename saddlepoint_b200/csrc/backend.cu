@@ -254,6 +254,7 @@ extern "C" int sp_ctx_create(int ordinal, sp_ctx **out) {
     }
     ctx->sms = prop.multiProcessorCount;
     ctx->name = prop.name;
+    keep_pool_memory(ordinal);
     ctx->cc_major = prop.major;
     ctx->cc_minor = prop.minor;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -282,6 +283,40 @@ extern "C" void sp_ctx_destroy(sp_ctx *ctx) {
 
 namespace sp {
 bool t_ctx_is(const sp_ctx *c) { return t_ctx == c; }
+
+// Device memory of problems and solvers comes from the device's stream-ordered pool,
+// allocated and released on the context's stream. The pool keeps what is released
+// (release threshold: unlimited), so a solve after a solve reuses mapped memory
+// instead of paying cudaMalloc/cudaFree's mapping, unmapping and device-wide
+// synchronisation again (0.1-1.2 s per 40M-nonzero solve, measured).
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    done[device] = true;
+}
+
+int dmalloc(void **p, size_t bytes) {
+    cudaStream_t st = t_ctx ? t_ctx->stream : nullptr;
+    cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 16), st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(SP_ERR_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+    }
+    return SP_OK;
+}
+
+void dfree(void *p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
+}
 int enter(sp_ctx *ctx) {
     if (!ctx) return SP_ERR_INVALID;
     set_current_ctx(ctx);
@@ -379,11 +414,13 @@ int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32) {
     }
     std::vector<Tile> tiles = build_tiles(h->row_ptr, h->nrows);
     d->ntiles = (int)tiles.size();
-    size_t nz = (size_t)std::max<int64_t>(h->nnz, 1);
-    SP_CUDA_TRY(cudaMalloc(&d->rp, sizeof(int) * (h->nrows + 1)));
-    SP_CUDA_TRY(cudaMalloc(&d->ci, sizeof(int) * nz));
-    SP_CUDA_TRY(cudaMalloc(&d->v, sizeof(double) * nz));
-    SP_CUDA_TRY(cudaMalloc(&d->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
+    d->nlong = count_long_tiles(tiles);
+    size_t nz = (size_t)std::max<int64_t>(h->nnz, 1) + CSR_PAD;
+    int rc;
+    if ((rc = dmalloc((void **)&d->rp, sizeof(int) * (h->nrows + 1 + CSR_PAD))) ||
+        (rc = dmalloc((void **)&d->ci, sizeof(int) * nz)) || (rc = dmalloc((void **)&d->v, sizeof(double) * nz)) ||
+        (rc = dmalloc((void **)&d->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1))))
+        return rc;
     SP_CUDA_TRY(cudaMemcpyAsync(d->rp, rp32.data(), sizeof(int) * (h->nrows + 1), cudaMemcpyHostToDevice, ctx->stream));
     if (h->nnz) {
         SP_CUDA_TRY(cudaMemcpyAsync(d->ci, h->col_idx, sizeof(int) * h->nnz, cudaMemcpyHostToDevice, ctx->stream));
@@ -393,30 +430,27 @@ int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32) {
         SP_CUDA_TRY(cudaMemcpyAsync(d->tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice,
                                     ctx->stream));
     const std::vector<uint16_t> sched = build_schedule(h->row_ptr, h->nrows, tiles);
-    SP_CUDA_TRY(cudaMalloc(&d->sched, sizeof(uint16_t) * std::max<int64_t>(h->nrows, 1)));
+    if ((rc = dmalloc((void **)&d->sched, sizeof(uint16_t) * (std::max<int64_t>(h->nrows, 1) + CSR_PAD)))) return rc;
     if (h->nrows)
         SP_CUDA_TRY(cudaMemcpyAsync(d->sched, sched.data(), sizeof(uint16_t) * h->nrows, cudaMemcpyHostToDevice,
                                     ctx->stream));
     if (want_f32) {
-        SP_CUDA_TRY(cudaMalloc(&d->v32, sizeof(float) * nz));
+        if ((rc = dmalloc((void **)&d->v32, sizeof(float) * nz))) return rc;
     }
     // the host vectors die with this call
     SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return SP_OK;
 }
 
-void free_csr(DevCsr *d) {
-    cudaFree(d->rp);
-    cudaFree(d->ci);
-    cudaFree(d->v);
-    cudaFree(d->v32);
-    cudaFree(d->tiles);
-    cudaFree(d->sched);
+void free_csr(DevCsr *d, cudaStream_t st) {
+    for (void *p : {(void *)d->rp, (void *)d->ci, (void *)d->v, (void *)d->v32, (void *)d->tiles, (void *)d->sched})
+        dfree(p, st);
     *d = DevCsr{};
 }
 
 int upload_vec(sp_ctx *ctx, double **d, const double *h, int64_t n) {
-    SP_CUDA_TRY(cudaMalloc(d, sizeof(double) * std::max<int64_t>(n, 1)));
+    int rc = dmalloc((void **)d, sizeof(double) * (std::max<int64_t>(n, 1) + CSR_PAD));
+    if (rc) return rc;
     if (n) SP_CUDA_TRY(cudaMemcpyAsync(*d, h, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
     return SP_OK;
 }
@@ -464,9 +498,10 @@ extern "C" void sp_problem_free(sp_problem *p) {
     if (!p) return;
     cudaSetDevice(p->ctx->device);
     cudaStreamSynchronize(p->ctx->stream);
-    free_csr(&p->a);
-    free_csr(&p->at);
-    for (double *v : {p->c, p->lc, p->uc, p->lv, p->uv, p->pf, p->df}) cudaFree(v);
+    free_csr(&p->a, p->ctx->stream);
+    free_csr(&p->at, p->ctx->stream);
+    for (double *v : {p->c, p->lc, p->uc, p->lv, p->uv, p->pf, p->df}) dfree(v, p->ctx->stream);
+    cudaStreamSynchronize(p->ctx->stream);
     delete p;
 }
 

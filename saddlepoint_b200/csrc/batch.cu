@@ -78,8 +78,6 @@ static std::mutex g_tune_mu;
 int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out,
                  bool tune);
 
-constexpr double HANDOFF_MIN_US = 20.0;
-
 int calibrate(sp_ctx *ctx, TuneTable *T) {
     // reference LPs: the random LP recipe, m from 60 to 2000, n = 2m, 3-8 nonzeros per column
     const int ms[] = {60, 180, 540, 2000};
@@ -108,6 +106,7 @@ int calibrate(sp_ctx *ctx, TuneTable *T) {
         A2.count = 1;
         A2.order = d_one;
         A2.base.tolerance = 0.0;  // never converged: every run takes exactly its iterations
+        A2.handoff_ns = 0;
         A2.power_iterations = std::min<unsigned long long>(A2.power_iterations, 4);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
@@ -184,24 +183,6 @@ int tune_variants(sp_batch *b) {
         for (auto &I : inst)
             I.variant =
                 estimate(VARIANT_TILES, I.nnz) <= estimate(VARIANT_LANES, I.nnz) ? VARIANT_TILES : VARIANT_LANES;
-        // Hand-off budgets: an instance whose iterations would hold its CTA for more
-        // than SP_BATCH_HANDOFF_S seconds stops there (at a check iteration) and is
-        // solved again by the single-LP solver. Only instances slower per iteration
-        // inside the kernel than HANDOFF_MIN_US (SP_BATCH_HANDOFF_MIN_US) get one: for
-        // the others the single-LP solver, bound by its launch latency, would be no
-        // faster. A budget is a multiple of check_every and at least 16 of them.
-        double handoff_s = 4.0, min_us = HANDOFF_MIN_US;
-        if (const char *env = getenv("SP_BATCH_HANDOFF_S")) handoff_s = atof(env);
-        if (const char *env = getenv("SP_BATCH_HANDOFF_MIN_US")) min_us = atof(env);
-        const unsigned long long E = b->params.check_every ? b->params.check_every : 64;
-        for (auto &I : inst) {
-            I.budget = 0;
-            const double us = estimate(I.variant, I.nnz);
-            if (handoff_s > 0 && us > min_us) {
-                const unsigned long long it = (unsigned long long)(handoff_s * 1e6 / us);
-                I.budget = std::max<unsigned long long>(16 * E, it / E * E);
-            }
-        }
     } else {
         for (auto &I : inst) I.variant = forced;
     }
@@ -262,17 +243,13 @@ int download_instance(const sp_batch *b, int i, HostLp *h) {
     return SP_OK;
 }
 
-// Solves the instances that stopped at their hand-off budget again with sp_solve,
+// Solves the instances the kernel stopped for the hand-off again with sp_solve,
 // up to eight at a time, each on a context (stream) of its own, and writes their
 // results and solutions where the kernel's would have gone.
 int hand_off(sp_batch *b, std::vector<sp_batch_result> &res) {
     std::vector<int> todo;
-    for (int i = 0; i < b->count; ++i) {
-        const BatchInst &I = b->inst[i];
-        if (I.budget && I.budget < b->params.max_iterations && res[i].status == SP_STATUS_ITERATION_LIMIT &&
-            res[i].iterations >= I.budget)
-            todo.push_back(i);
-    }
+    for (int i = 0; i < b->count; ++i)
+        if (res[i].handed_off == 2) todo.push_back(i);
     if (todo.empty()) return SP_OK;
     // the largest first, so the longest solves start early
     std::stable_sort(todo.begin(), todo.end(), [&](int a, int c) { return b->inst[a].nnz > b->inst[c].nnz; });
@@ -551,6 +528,12 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
             return bail(rc, "out of device memory");
     }
     if ((rc = balloc(b, &A.res, count))) return bail(rc, "out of device memory");
+    if ((rc = balloc(b, &A.drain_ns, 1))) return bail(rc, "out of device memory");
+    {
+        double handoff_s = 2.0;
+        if (const char *env = getenv("SP_BATCH_HANDOFF_S")) handoff_s = atof(env);
+        A.handoff_ns = handoff_s > 0 ? (unsigned long long)(handoff_s * 1e9) : 0ull;
+    }
     DevParams dp{};
     dp.tolerance = P.tolerance;
     dp.infeasibility_tolerance = P.infeasibility_tolerance;
@@ -600,6 +583,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
     cudaMemcpyAsync(av, av0, sizeof(double) * nz, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(tv, tv0, sizeof(double) * nz, cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+    cudaMemsetAsync(A.drain_ns, 0, sizeof(unsigned long long), st);
     k_batch<NT><<<b->grid, NT, smem, st>>>(A);
     SP_CUDA_TRY(cudaStreamEndCapture(st, &g));
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);

@@ -32,7 +32,6 @@ struct BatchInst {
     int nta, ntt;          // tiles of A' and A'ᵀ
     double c0;
     int maximize, pad2;
-    unsigned long long budget;  // iteration cap inside the batch (0: the solve's own limit)
 };
 
 enum : int { VARIANT_LANES = 0, VARIANT_TILES = 1 };
@@ -42,6 +41,11 @@ struct BatchArgs {
     const int *order;  // processing order (largest first)
     int count;
     int *counter;
+    // The tail hand-off: once every instance has been claimed (drain_ns: when, 0 before),
+    // an instance still running handoff_ns later stops at its next check and is
+    // finished by the single-LP solver on the host's side (0: never).
+    unsigned long long *drain_ns;
+    unsigned long long handoff_ns;
     const int *a_rp, *a_ci, *t_rp, *t_ci;
     double *a_v, *t_v;
     float *a_v32, *t_v32;
@@ -59,6 +63,18 @@ struct BatchArgs {
     double pc_alpha, step_size_factor;
     int mixed;
 };
+
+// Thread 0, after a check that did not end the solve: stop for the hand-off when the
+// queue drained more than handoff_ns ago (the instance is a straggler of the tail).
+__device__ __forceinline__ void tail_handoff(const BatchArgs &A, DevState &st) {
+    if (st.done || A.handoff_ns == 0) return;
+    const unsigned long long drained = *reinterpret_cast<volatile unsigned long long *>(A.drain_ns);
+    if (drained && global_ns() - drained > A.handoff_ns) {
+        st.done = 1;
+        st.status = SP_STATUS_ITERATION_LIMIT;
+        st.handoff = 1;
+    }
+}
 
 template <int BT, int K>
 __device__ __forceinline__ void bsum(double (&v)[K], double *sh) {
@@ -279,6 +295,7 @@ __device__ void batch_tiles_solve(const BatchArgs &A, const BatchInst &I, const 
             bool bad = false;
             sp_check_record rec;
             check_decide(&st, &prm, P, D, T, st.k, st.total + 1, &bad, &rec);
+            tail_handoff(A, st);
         }
         __syncthreads();
         if (st.done) break;
@@ -425,7 +442,6 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         bc[0] = bs;
         bc[1] = os;
         prm = A.base;
-        if (I.budget && I.budget < prm.max_iterations) prm.max_iterations = I.budget;
         prm.b_norm = fbn(olc, ouc);
         prm.c_norm = n2(oc);
         prm.c0 = I.c0;
@@ -751,6 +767,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
             bool bad = false;
             sp_check_record rec;
             check_decide(&st, &prm, P, D, T, k, total, &bad, &rec);
+            tail_handoff(A, st);
         }
         __syncthreads();
         if (st.done) break;
@@ -786,7 +803,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         r.iterations = st.total;
         r.restarts = st.restarts;
         r.lanes_per_row = I.variant == VARIANT_TILES ? 0 : I.lanes_a * 100 + I.lanes_t;
-        r.handed_off = 0;
+        r.handed_off = st.handoff ? 2 : 0;  // 2: the host finishes it
         A.res[id] = r;
     }
     __syncthreads();
@@ -805,7 +822,10 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs A) {
         __syncthreads();
         const int slot = next;
         __syncthreads();
-        if (slot >= A.count) return;
+        if (slot >= A.count) {
+            if (threadIdx.x == 0) atomicCAS(A.drain_ns, 0ull, global_ns());
+            return;
+        }
         batch_solve_one<BT>(A, A.order[slot], sh, st, prm, bc, dsm);
     }
 }

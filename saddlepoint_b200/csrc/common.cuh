@@ -123,14 +123,19 @@ struct DevState {
     unsigned long long trace_len;
     // mixed form: best relative KKT error of the FP32 phase and checks since it improved
     double mx_best;
-    int mx_since, pad1;
+    int mx_since;
+    int handoff;  // batched form: stopped for the single-LP solver
 };
 
 // Mixed form: checks without a 10% gain in the relative KKT error after which the
 // FP32 phase is taken to have stalled at its precision and the SpMV moves to FP64.
 constexpr int MIXED_STALL_CHECKS = 40;
 
-enum : int { ERR_NONE = 0, ERR_NUMERICAL_POWER = 1, ERR_NUMERICAL_ITERATES = 2 };
+enum : int { ERR_NONE = 0, ERR_NUMERICAL_POWER = 1, ERR_NUMERICAL_ITERATES = 2, ERR_PIPELINE_STALL = 3 };
+
+// Elements of slack after the last row pointer / nonzero / vector entry of the
+// arrays the stream engine stages: a bulk copy rounds its range out to 16 bytes.
+constexpr int CSR_PAD = 16;
 
 // ---- host-side error plumbing ----
 

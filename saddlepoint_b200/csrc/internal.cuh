@@ -37,12 +37,18 @@ struct DevCsr {
     Tile *tiles = nullptr;
     int ntiles = 0;
     uint16_t *sched = nullptr;  // row schedule of every tile (build_schedule)
+    int nlong = 0;              // leading tiles that hold one row longer than TILE_NNZ
 };
 
 int enter(sp_ctx *ctx);
 bool t_ctx_is(const sp_ctx *c);
 int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32);
-void free_csr(DevCsr *d);
+void free_csr(DevCsr *d, cudaStream_t st);
+// Stream-ordered device memory from the device's pool (see backend.cu): allocated on
+// the calling thread's context stream, released on `st`.
+int dmalloc(void **p, size_t bytes);
+void dfree(void *p, cudaStream_t st);
+void keep_pool_memory(int device);
 int upload_vec(sp_ctx *ctx, double **d, const double *h, int64_t n);
 void launch_spmv(sp_ctx *ctx, const DevCsr &A, const double *x, double *out, cudaStream_t s);
 

@@ -8,8 +8,11 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "control.cuh"
@@ -233,21 +236,55 @@ __global__ void k_scale_vectors(const double *c, const double *lc, const double 
 // The four norms the solve needs, each a sequential sum from -0.0 in index order,
 // as the reference computes them (scaling.rs:186-201): finite_bound_norm and norm2
 // of the scaled bounds and objective, and of the original ones (solver.rs:317-318).
-// One thread per norm: this runs once per solve.
-__global__ void k_seq_norms(const double *lc, const double *uc, int64_t m, const double *c, int64_t n, double *out,
-                            int which) {
-    if (threadIdx.x != 0) return;
-    double s = -0.0;
-    if (which == 0) {
-        for (int64_t i = 0; i < m; ++i) {
-            const double l = isfinite(lc[i]) ? lc[i] : 0.0;
-            const double u = isfinite(uc[i]) ? uc[i] : 0.0;
-            s += (l == u) ? l * l : l * l + u * u;
+// Each norm is one sequential sum in index order, added by thread 0 of its block
+// while the other threads stage the next chunk in shared memory (the add chain, not
+// the loads, sets the pace). Block b computes norm b: the bound and cost norms of
+// the original problem (norms[2], norms[3]) and of the scaled one (norms[0],
+// norms[1]).
+constexpr int SEQ_CHUNK = 1024;
+
+__global__ void __launch_bounds__(NT) k_seq_norms(const double *olc, const double *ouc, const double *oc,
+                                                  const double *lc, const double *uc, const double *c, int64_t m,
+                                                  int64_t n, double *norms) {
+    __shared__ double sa[2][SEQ_CHUNK], sb[2][SEQ_CHUNK];
+    const int which = blockIdx.x & 1;  // 0: bound norm over m rows, 1: cost norm over n columns
+    const bool orig = blockIdx.x < 2;
+    const double *a = which == 0 ? (orig ? olc : lc) : (orig ? oc : c);
+    const double *b = orig ? ouc : uc;
+    const int64_t len = which == 0 ? m : n;
+    const int64_t nchunks = (len + SEQ_CHUNK - 1) / SEQ_CHUNK;
+    auto stage = [&](int64_t k, int buf) {  // threads 1..NT-1
+        const int64_t base = k * SEQ_CHUNK;
+        for (int i = threadIdx.x - 1; i < SEQ_CHUNK; i += NT - 1) {
+            const int64_t e = base + i;
+            if (e < len) {
+                sa[buf][i] = a[e];
+                if (which == 0) sb[buf][i] = b[e];
+            }
         }
-    } else {
-        for (int64_t j = 0; j < n; ++j) s += c[j] * c[j];
+    };
+    if (threadIdx.x > 0 && nchunks > 0) stage(0, 0);
+    __syncthreads();
+    double s = -0.0;
+    for (int64_t k = 0; k < nchunks; ++k) {
+        const int buf = (int)(k & 1);
+        if (threadIdx.x == 0) {
+            const int cnt = (int)min((int64_t)SEQ_CHUNK, len - k * SEQ_CHUNK);
+            if (which == 0) {
+                for (int i = 0; i < cnt; ++i) {
+                    const double l = isfinite(sa[buf][i]) ? sa[buf][i] : 0.0;
+                    const double u = isfinite(sb[buf][i]) ? sb[buf][i] : 0.0;
+                    s += (l == u) ? l * l : l * l + u * u;
+                }
+            } else {
+                for (int i = 0; i < cnt; ++i) s += sa[buf][i] * sa[buf][i];
+            }
+        } else if (k + 1 < nchunks) {
+            stage(k + 1, buf ^ 1);
+        }
+        __syncthreads();
     }
-    out[0] = sqrt(s);
+    if (threadIdx.x == 0) norms[(orig ? 2 : 0) + which] = sqrt(s);
 }
 
 __global__ void k_rescale(double *lc, double *uc, double *lv, double *uv, double *c, const double *norms, int64_t m,
@@ -339,10 +376,11 @@ int grid_of(const sp_ctx *ctx, int64_t n, int per_thread_items = 1) {
     return (int)std::max<int64_t>(1, std::min(b, cap));
 }
 
+// Device arrays carry CSR_PAD elements of slack: the bulk copies of the stream
+// engine round their ranges out to 16-byte boundaries.
 template <class T>
 int dalloc(T **p, int64_t n) {
-    SP_CUDA_TRY(cudaMalloc(p, sizeof(T) * std::max<int64_t>(n, 1)));
-    return SP_OK;
+    return dmalloc((void **)p, sizeof(T) * (std::max<int64_t>(n, 1) + CSR_PAD));
 }
 
 }  // namespace
@@ -426,12 +464,106 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
     return o;
 }
 
-// Launches the primal pass of iteration i with the given role.
+// The stream engine kernels of one FUSED op: one CTA per SM. Variants differ in
+// the gatherer warps (count, loads in flight per lane, register or cp.async
+// gathers); choose_engines() picks one per pass when a solver is created.
+enum StreamVariant : int { SV_LDG4 = 0, SV_LDG8, SV_LDG8B16, SV_LDG12, SV_CP4, SV_COUNT };
+
+template <class Op>
+struct StreamKernel {
+    static constexpr size_t smem = StreamLayout<Op>::total;
+    static std::atomic<int> ready[64];
+    template <int GW, bool LDG, int B>
+    static int prepare_one() {
+        SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_stream<Op, GW, LDG, B>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int b = 0;
+        SP_CUDA_TRY(
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_stream<Op, GW, LDG, B>, stream_threads(GW), smem));
+        if (b < 1) return fail(SP_ERR_CUDA, "stream engine kernel cannot be resident");
+        return SP_OK;
+    }
+    // Runs before any graph capture: opts every variant in to its shared memory.
+    static int prepare(int dev) {
+        if (dev < 0 || dev >= 64) return fail(SP_ERR_INVALID, "device ordinal out of range");
+        if (ready[dev].load()) return SP_OK;
+        int rc;
+        if ((rc = prepare_one<4, true, 8>()) || (rc = prepare_one<8, true, 8>()) || (rc = prepare_one<8, true, 16>()) ||
+            (rc = prepare_one<12, true, 8>()) || (rc = prepare_one<4, false, 1>()))
+            return rc;
+        ready[dev].store(1);
+        return SP_OK;
+    }
+    template <int GW, bool LDG, int B>
+    static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op) {
+        k_stream<Op, GW, LDG, B><<<grid, stream_threads(GW), smem, st>>>(M.ntiles, M.nlong, op);
+    }
+    static void launch(const sp_ctx *ctx, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctx->sms, M.ntiles));
+        switch (variant) {
+        case SV_LDG4: go<4, true, 8>(grid, M, st, op); break;
+        case SV_LDG8: go<8, true, 8>(grid, M, st, op); break;
+        case SV_LDG8B16: go<8, true, 16>(grid, M, st, op); break;
+        case SV_LDG12: go<12, true, 8>(grid, M, st, op); break;
+        default: go<4, false, 1>(grid, M, st, op); break;
+        }
+    }
+};
+template <class Op>
+std::atomic<int> StreamKernel<Op>::ready[64];
+
+using StreamP64 = StreamKernel<PrimalPass<false, 0>>;
+using StreamP32 = StreamKernel<PrimalPass<true, 0>>;
+using StreamD64 = StreamKernel<DualPass<false, 0>>;
+using StreamD32 = StreamKernel<DualPass<true, 0>>;
+
+// Which engine runs each MID pass (-1: the tile engine, else a stream variant). The
+// defaults are the faster on the 40M power-law LP: the stream engine for the primal
+// pass in both precisions (8 gatherer warps, 16 loads in flight per lane) and for the
+// FP32 dual pass (cp.async gatherers), the tile engine for the FP64 dual pass.
+// SP_PASS_ENGINE=tiles|stream overrides all four; SP_STREAM_GATHER then names the
+// variant.
+int choose_engines(sp_solver *s) {
+    s->sv_p64 = SV_LDG8B16;
+    s->sv_p32 = SV_LDG8B16;
+    s->sv_d64 = -1;
+    s->sv_d32 = SV_CP4;
+    const char *eng = getenv("SP_PASS_ENGINE");
+    if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
+    if (eng && !strcmp(eng, "stream")) {
+        int v = SV_LDG8;
+        const char *gv = getenv("SP_STREAM_GATHER");
+        const char *names[SV_COUNT] = {"ldg4", "ldg8", "ldg8b16", "ldg12", "cp4"};
+        for (int k = 0; gv && k < SV_COUNT; ++k)
+            if (!strcmp(gv, names[k])) v = k;
+        s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = v;
+    }
+    const int dev = s->ctx->device;
+    int rc;
+    if (s->sv_p64 >= 0 && (rc = StreamP64::prepare(dev))) return rc;
+    if (s->sv_d64 >= 0 && (rc = StreamD64::prepare(dev))) return rc;
+    if (s->mixed && s->sv_p32 >= 0 && (rc = StreamP32::prepare(dev))) return rc;
+    if (s->mixed && s->sv_d32 >= 0 && (rc = StreamD32::prepare(dev))) return rc;
+    return SP_OK;
+}
+
+// Launches the primal pass of iteration i with the given role. MID iterations go
+// through the stream engine when it is on (in the mixed form one launch per
+// precision; the one that does not match the device state returns at once).
 void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     const SolverPtrs p = ptrs_of(s);
     const int g = s->AT.ntiles;
     if (g == 0) return;
     const size_t sm = smem_P();
+    if (role == ROLE_MID && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
+        if (s->mixed) {
+            if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
+            else k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role));
+        }
+        if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
+        else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
+        return;
+    }
     if (s->mixed) {
         if (role == ROLE_MID)
             k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
@@ -458,6 +590,16 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
     const int g = s->A.ntiles;
     if (g == 0) return;
     const size_t sm = smem_D();
+    if (role == ROLE_MID && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
+        const size_t s1 = tile_smem_bytes<1, double>();
+        if (s->mixed) {
+            if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
+            else k_tiles_any<<<g, NT, s1, st>>>(mkD<true, 0>(p, i, role));
+        }
+        if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
+        else k_tiles_any<<<g, NT, s1, st>>>(mkD<false, 0>(p, i, role));
+        return;
+    }
     if (s->mixed) {
         if (role == ROLE_MID)
             k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
@@ -565,13 +707,15 @@ void solver_release(sp_solver *s) {
     cudaStreamSynchronize(s->ctx->stream);
     for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
     for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
-    free_csr(&s->A);
-    free_csr(&s->AT);
+    cudaStream_t fst = s->ctx->stream;
+    free_csr(&s->A, fst);
+    free_csr(&s->AT, fst);
     void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
                     s->aty, s->xbar32, s->y32, s->pk, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
                     s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,
                     s->out_x, s->out_y};
-    for (void *b : bufs) cudaFree(b);
+    for (void *b : bufs) dfree(b, fst);
+    cudaStreamSynchronize(fst);
     cudaFreeHost(s->h_st);
     delete s;
 }
@@ -623,18 +767,15 @@ int scale_on_device(sp_solver *s, const sp_lp *lp) {
         (rc = upload_vec(ctx, &ouv, lp->uv, n)))
         return rc;
     // norms of the original problem (solver.rs:317-318)
-    k_seq_norms<<<1, 32, 0, st>>>(olc, ouc, m, oc, n, s->norms + 2, 0);
-    k_seq_norms<<<1, 32, 0, st>>>(olc, ouc, m, oc, n, s->norms + 3, 1);
     k_scale_vectors<<<std::max(gm, gn), NT, 0, st>>>(oc, olc, ouc, olv, ouv, s->row_scale, s->col_scale, s->c, s->lc,
                                                      s->uc, s->lv, s->uv, m, n);
-    k_seq_norms<<<1, 32, 0, st>>>(s->lc, s->uc, m, s->c, n, s->norms + 0, 0);
-    k_seq_norms<<<1, 32, 0, st>>>(s->lc, s->uc, m, s->c, n, s->norms + 1, 1);
+    k_seq_norms<<<4, NT, 0, st>>>(olc, ouc, oc, s->lc, s->uc, s->c, m, n, s->norms);
     k_rescale<<<std::max(gm, gn), NT, 0, st>>>(s->lc, s->uc, s->lv, s->uv, s->c, s->norms, m, n,
                                                P.bound_objective_rescaling, s->scales);
     k_factors<<<std::max(gm, gn), NT, 0, st>>>(s->row_scale, s->col_scale, s->scales, s->pf, s->df, m, n);
     SP_CUDA_TRY(cudaGetLastError());
     SP_CUDA_TRY(cudaStreamSynchronize(st));
-    for (double *b : {r, c, ones_m, ones_n, oc, olc, ouc, olv, ouv}) cudaFree(b);
+    for (double *b : {r, c, ones_m, ones_n, oc, olc, ouc, olv, ouv}) dfree(b, st);
     return SP_OK;
 }
 
@@ -663,20 +804,21 @@ int transpose_on_device(sp_solver *s) {
     SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp, s->A.ci, keys_out, perm_in, perm_out, (int)nnz, 0, bits,
                                                 st));
     void *tmp = nullptr;
-    SP_CUDA_TRY(cudaMalloc(&tmp, std::max<size_t>(temp, 1)));
+    if ((rc = dmalloc(&tmp, std::max<size_t>(temp, 1)))) return rc;
     SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, s->A.ci, keys_out, perm_in, perm_out, (int)nnz, 0, bits, st));
     k_rowptr_from_sorted<<<grid_of(ctx, n + 1), NT, 0, st>>>(keys_out, nnz, n, T.rp);
     k_gather_transpose<<<grid_of(ctx, nnz), NT, 0, st>>>(perm_out, row_of, s->A.v, T.ci, T.v, nnz);
     SP_CUDA_TRY(cudaGetLastError());
     SP_CUDA_TRY(cudaStreamSynchronize(st));
-    for (void *b : {(void *)row_of, (void *)keys_out, (void *)perm_in, (void *)perm_out, tmp}) cudaFree(b);
+    for (void *b : {(void *)row_of, (void *)keys_out, (void *)perm_in, (void *)perm_out, tmp}) dfree(b, st);
     // tile plan of A'ᵀ from its row pointers
     std::vector<int> rp32(n + 1);
     SP_CUDA_TRY(cudaMemcpy(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
     std::vector<int64_t> rp64(rp32.begin(), rp32.end());
     std::vector<Tile> tiles = build_tiles(rp64.data(), n);
     T.ntiles = (int)tiles.size();
-    SP_CUDA_TRY(cudaMalloc(&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
+    T.nlong = count_long_tiles(tiles);
+    if ((rc = dmalloc((void **)&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)))) return rc;
     if (!tiles.empty())
         SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
     const std::vector<uint16_t> sched = build_schedule(rp64.data(), n, tiles);
@@ -696,8 +838,25 @@ int validate_lp(const sp_lp *lp) {  // LpProblem::validate (problem.rs:166-194)
         if (std::isnan(lp->lc[i]) || std::isnan(lp->uc[i])) return fail(SP_ERR_PROBLEM, "constraint bound is NaN");
         if (lp->lc[i] > lp->uc[i]) return fail(SP_ERR_PROBLEM, "constraint has lower bound above upper bound");
     }
-    for (int64_t k = 0; k < lp->a.nnz; ++k)
-        if (std::isnan(lp->a.values[k])) return fail(SP_ERR_PROBLEM, "coefficient is NaN");
+    // the coefficient scan is the long one: split it over host threads
+    const int64_t nnz = lp->a.nnz;
+    const int workers = (int)std::max<int64_t>(1, std::min<int64_t>(16, nnz >> 20));
+    std::atomic<int> nan_found{0};
+    auto scan = [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k)
+            if (std::isnan(lp->a.values[k])) {
+                nan_found.store(1);
+                return;
+            }
+    };
+    if (workers == 1) {
+        scan(0, nnz);
+    } else {
+        std::vector<std::thread> th;
+        for (int w = 0; w < workers; ++w) th.emplace_back(scan, nnz * w / workers, nnz * (w + 1) / workers);
+        for (auto &t : th) t.join();
+    }
+    if (nan_found.load()) return fail(SP_ERR_PROBLEM, "coefficient is NaN");
     return SP_OK;
 }
 
@@ -857,6 +1016,7 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     if ((rc = dalloc(&s->d_trace, s->trace_cap))) return cleanup(rc);
     SP_CUDA_TRY(cudaMallocHost(&s->h_st, sizeof(DevState) * (SolverLookahead + 2)));
     if ((rc = set_smem_limits())) return cleanup(rc);
+    if ((rc = choose_engines(s))) return cleanup(rc);
     // ‖A'‖₂ and η (solver.rs:316)
     if ((rc = sp_solver_reset(s))) return cleanup(rc);
     if ((rc = power_iteration(s))) return cleanup(rc);
@@ -1012,6 +1172,8 @@ extern "C" int sp_solver_solve(sp_solver *s, sp_solution_info *info) {
     last = s->h_st[0];
     s->solve_s = now_s() - t0;
     if (last.error == ERR_NUMERICAL_ITERATES) return fail(SP_ERR_NUMERICAL, "numerical breakdown: iterates are not finite");
+    if (last.error == ERR_PIPELINE_STALL)
+        return fail(SP_ERR_CUDA, "a bulk copy of the pass pipeline did not complete within one second");
     if (!last.done && !s->time_limited) s->time_limited = true;  // only reachable with an exhausted limit
     fill_info(s, last, info);
     return SP_OK;

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "control.cuh"
+#include "stream.cuh"
 #include "tiles.cuh"
 
 namespace sp {
@@ -115,6 +116,26 @@ struct PrimalPass {
         p.xa = MODE == 1 ? 0.0 : __ldcs(s.xa + j);
         return p;
     }
+    // The stream engine's view of the pass (FUSED only): the gathered vector, the
+    // product, the row inputs as arrays it stages (x, c, lv, uv, x_anchor) and the
+    // Pre read back from shared memory (p: row q of array 0).
+    using GT = VT;
+    __device__ __forceinline__ const GT *gvec() const {
+        if constexpr (LO) return s.y32;
+        else return s.y;
+    }
+    __device__ __forceinline__ ST mul(VT v, GT g) const { return v * g; }
+    static constexpr int NPRE = 5;
+    __device__ __forceinline__ const double *pre_array(int q) const {
+        return q == 0 ? s.x : q == 1 ? s.c : q == 2 ? s.lv : q == 3 ? s.uv : s.xa;
+    }
+    __device__ __forceinline__ Pre pre_smem(const double *p, int stride) const {
+        return Pre{p[0], p[stride], p[2 * stride], p[3 * stride], MODE == 1 ? 0.0 : p[4 * stride]};
+    }
+    __device__ void fault() const {
+        s.st->error = ERR_PIPELINE_STALL;
+        s.st->done = 1;
+    }
     __device__ __forceinline__ void row(int j, const double (&sum)[1], double *part, const Pre &in) const {
         const double aty = sum[0];
         const double xj = in.x;
@@ -209,6 +230,25 @@ struct DualPass {
         p.ya = __ldcs(s.ya + r);
         p.pf = MODE == 2 ? __ldcs(s.pf + r) : 0.0;
         return p;
+    }
+    // The stream engine's view of the pass (FUSED only): the gathered vector, the
+    // product and the row inputs it stages (y, lc, uc, y_anchor).
+    using GT = typename std::conditional<LO && MODE == 0, float, double>::type;
+    __device__ __forceinline__ const GT *gvec() const {
+        if constexpr (LO && MODE == 0) return s.xbar32;
+        else return s.xbar;
+    }
+    __device__ __forceinline__ ST mul(VT v, GT g) const { return ST(v * g); }
+    static constexpr int NPRE = 4;
+    __device__ __forceinline__ const double *pre_array(int q) const {
+        return q == 0 ? s.y : q == 1 ? s.lc : q == 2 ? s.uc : s.ya;
+    }
+    __device__ __forceinline__ Pre pre_smem(const double *p, int stride) const {
+        return Pre{p[0], p[stride], p[2 * stride], p[3 * stride], 0.0};
+    }
+    __device__ void fault() const {
+        s.st->error = ERR_PIPELINE_STALL;
+        s.st->done = 1;
     }
     __device__ __forceinline__ void row(int r, const double (&sum)[G], double *part, const Pre &in) const {
         const double a = sum[0], yi = in.y;

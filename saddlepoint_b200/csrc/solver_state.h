@@ -17,6 +17,8 @@ struct sp_solver {
     sp_ctx *ctx = nullptr;
     sp_solver_params prm{};
     int mixed = 0;
+    // engine of each MID pass: -1 the tile engine, else a stream-engine variant (stream.cuh)
+    int sv_p64 = -1, sv_p32 = -1, sv_d64 = -1, sv_d32 = -1;
     int64_t m = 0, n = 0, nnz = 0;
     double c0 = 0.0;
     int maximize = 0;

@@ -150,6 +150,13 @@ __device__ __forceinline__ const uint16_t *sched_of(const Op &op) {
     else return nullptr;
 }
 
+// Number of leading tiles of a plan that hold a single row longer than TILE_NNZ.
+inline int count_long_tiles(const std::vector<Tile> &tiles) {
+    int n = 0;
+    while (n < (int)tiles.size() && (int64_t)tiles[n].w - tiles[n].z > TILE_NNZ) ++n;
+    return n;
+}
+
 template <int G, class ST>
 constexpr size_t tile_smem_bytes() {
     return (size_t)G * TILE_NNZ * sizeof(ST) + (TILE_ROWS + 1) * sizeof(int);

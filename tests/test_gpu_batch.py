@@ -94,27 +94,33 @@ def test_batch_tile_variant_equals_the_solo_device_solve(batch_lps, gpu_backend,
 
 
 def test_batch_hand_off_gives_the_solo_device_solve(batch_lps, gpu_backend, monkeypatch):
-    """An instance that outruns its share of the persistent kernel is solved again from
-    the start by sp_solve: its result is the solo solve's, bit for bit. One that
-    converges within its budget stays in the kernel (afiro: 576 iterations)."""
-    monkeypatch.setenv("SP_BATCH_HANDOFF_S", "1e-9")  # every budget: 16 checks = 1024 iterations
-    monkeypatch.setenv("SP_BATCH_HANDOFF_MIN_US", "0")
+    """An instance the kernel stops for the hand-off (still running after the queue has
+    drained) is solved again from the start by sp_solve: its result is the solo solve's,
+    bit for bit. With a hand-off delay of zero every instance but the first to finish is a
+    straggler: the grid has one CTA per instance, and the first CTA to finish drains the
+    queue."""
+    monkeypatch.setenv("SP_BATCH_HANDOFF_S", "1e-9")
     lps = batch_lps[:5] + [netlib_lp("afiro"), netlib_lp("adlittle")]
     params = sp().SolverParams(tolerance=TOL)
     b = sp().BatchSolver(lps, params, gpu_backend)
     res, elapsed = b.solve()
     assert elapsed > 0
-    assert not res[5].handed_off and res[5].iterations <= 1024
-    assert res[6].handed_off
+    assert sum(r.handed_off for r in res) >= len(lps) - 1
     for i, (lp, r) in enumerate(zip(lps, res)):
         x, y = b.solution(i)
         if not r.handed_off:
             oracle.check(lp, x, y).verify(2 * TOL)
             continue
         solo = sp().solve(lp, params, gpu_backend)
-        assert r.iterations == solo.iterations and r.iterations > 1024, (i, r.iterations, solo.iterations)
+        assert r.iterations == solo.iterations, (i, r.iterations, solo.iterations)
         assert r.objective == solo.objective and r.status == int(solo.status)
         assert np.array_equal(x, solo.x) and np.array_equal(y, solo.y), i
+
+
+def test_batch_without_stragglers_hands_off_nothing(batch_lps, gpu_backend):
+    b = sp().BatchSolver(batch_lps[:8], sp().SolverParams(tolerance=TOL), gpu_backend)
+    res, _ = b.solve()
+    assert not any(r.handed_off for r in res)
 
 
 def test_batch_repeat_is_identical(batch_lps, gpu_backend):
