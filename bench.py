@@ -270,13 +270,13 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
 
-    def roofline(meas):
+    def roofline(meas, form=""):
         k = meas["kernels"]
         dom = max(k, key=lambda name: k[name]["avg_ms"])
         d = k[dom]
         achieved = d["bytes_per_launch"] / (d["avg_ms"] * 1e-3) / 1e9 if d["avg_ms"] > 0 else 0.0
         return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(dom),
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(dom + form),
                 "bytes_per_launch": d["bytes_per_launch"], "avg_launch_ms": d["avg_ms"],
                 "launches_timed": d["launches_timed"],
                 "other": {name: {"achieved_gbs": k[name]["bytes_per_launch"] / (k[name]["avg_ms"] * 1e-3) / 1e9
@@ -338,9 +338,11 @@ def run_ours(args):
             "mixed": {"iter_per_s": mixed_value, "ms_per_step": mix["ms"] / args.steps,
                       "gb_per_iteration": mix["bytes_per_iteration"] / 1e9,
                       "hbm_gbs_whole_iteration": mix["bytes_per_iteration"] * mixed_value / n / 1e9,
-                      "roofline": roofline(mix), "clocks": mix["clocks"],
+                      "roofline": roofline(mix, "_mixed"), "clocks": mix["clocks"],
                       "speedup_vs_fp64": mixed_value / value,
-                      "note": "FP32 SpMV through the timed window (tolerance 1e-12 keeps it from switching)"},
+                      "fp64_from_iteration": mix["fp64_from_iteration"],
+                      "note": "tolerances of 0: no check ends the solve or moves the SpMV to FP64 by "
+                              "accuracy; fp64_from_iteration > 0 would show the stall rule's switch"},
         },
         "setup_s": f64["setup_s"],
     }
