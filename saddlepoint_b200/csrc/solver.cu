@@ -464,22 +464,24 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
     return o;
 }
 
-// The stream engine kernels of one FUSED op: one CTA per SM. Variants differ in
-// the gatherer warps (count, loads in flight per lane, register or cp.async
-// gathers); choose_engines() picks one per pass when a solver is created.
-enum StreamVariant : int { SV_LDG4 = 0, SV_LDG8, SV_LDG8B16, SV_LDG12, SV_CP4, SV_COUNT };
+// The stream engine kernels of one FUSED op: one CTA per SM. Variants differ in the
+// gatherer warps (count, loads in flight per lane, register or cp.async gathers) and
+// in the slot count; choose_engines() picks one per pass when a solver is created.
+enum StreamVariant : int { SV_LDG4 = 0, SV_LDG4_DEEP, SV_LDG8B16, SV_LDG8B16_DEEP, SV_CP4, SV_COUNT };
 
 template <class Op>
 struct StreamKernel {
-    static constexpr size_t smem = StreamLayout<Op>::total;
+    template <bool LDG, bool DEEP>
+    static constexpr size_t smem_of() { return StreamLayout<Op, !LDG, DEEP>::total; }
     static std::atomic<int> ready[64];
-    template <int GW, bool LDG, int B>
+    template <int GW, bool LDG, int B, bool DEEP>
     static int prepare_one() {
-        SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_stream<Op, GW, LDG, B>,
+        constexpr size_t smem = smem_of<LDG, DEEP>();
+        SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_stream<Op, GW, LDG, B, DEEP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int b = 0;
-        SP_CUDA_TRY(
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_stream<Op, GW, LDG, B>, stream_threads(GW), smem));
+        SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_stream<Op, GW, LDG, B, DEEP>,
+                                                                  stream_threads(GW), smem));
         if (b < 1) return fail(SP_ERR_CUDA, "stream engine kernel cannot be resident");
         return SP_OK;
     }
@@ -488,24 +490,25 @@ struct StreamKernel {
         if (dev < 0 || dev >= 64) return fail(SP_ERR_INVALID, "device ordinal out of range");
         if (ready[dev].load()) return SP_OK;
         int rc;
-        if ((rc = prepare_one<4, true, 8>()) || (rc = prepare_one<8, true, 8>()) || (rc = prepare_one<8, true, 16>()) ||
-            (rc = prepare_one<12, true, 8>()) || (rc = prepare_one<4, false, 1>()))
+        if ((rc = prepare_one<4, true, 8, false>()) || (rc = prepare_one<4, true, 8, true>()) ||
+            (rc = prepare_one<8, true, 16, false>()) || (rc = prepare_one<8, true, 16, true>()) ||
+            (rc = prepare_one<4, false, 1, false>()))
             return rc;
         ready[dev].store(1);
         return SP_OK;
     }
-    template <int GW, bool LDG, int B>
+    template <int GW, bool LDG, int B, bool DEEP>
     static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op) {
-        k_stream<Op, GW, LDG, B><<<grid, stream_threads(GW), smem, st>>>(M.ntiles, M.nlong, op);
+        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op);
     }
     static void launch(const sp_ctx *ctx, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctx->sms, M.ntiles));
         switch (variant) {
-        case SV_LDG4: go<4, true, 8>(grid, M, st, op); break;
-        case SV_LDG8: go<8, true, 8>(grid, M, st, op); break;
-        case SV_LDG8B16: go<8, true, 16>(grid, M, st, op); break;
-        case SV_LDG12: go<12, true, 8>(grid, M, st, op); break;
-        default: go<4, false, 1>(grid, M, st, op); break;
+        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op); break;
+        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op); break;
+        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op); break;
+        case SV_LDG8B16_DEEP: go<8, true, 16, true>(grid, M, st, op); break;
+        default: go<4, false, 1, false>(grid, M, st, op); break;
         }
     }
 };
@@ -518,22 +521,24 @@ using StreamD64 = StreamKernel<DualPass<false, 0>>;
 using StreamD32 = StreamKernel<DualPass<true, 0>>;
 
 // Which engine runs each MID pass (-1: the tile engine, else a stream variant). The
-// defaults are the faster on the 40M power-law LP: the stream engine for the primal
-// pass in both precisions (8 gatherer warps, 16 loads in flight per lane) and for the
-// FP32 dual pass (cp.async gatherers), the tile engine for the FP64 dual pass.
+// defaults are the fastest measured on the 40M power-law LP (ms per launch): FP64
+// primal on the stream engine, 4 register-gatherer warps, 4 slots (0.255; tile engine
+// 0.301); FP64 dual on the tile engine (0.235; stream 0.300); FP32 primal on the
+// stream engine, 4 gatherer warps, 4 slots (0.247; tile 0.285); FP32 dual on the
+// stream engine, 8 gatherer warps x 16 loads in flight (0.222; tile 0.242).
 // SP_PASS_ENGINE=tiles|stream overrides all four; SP_STREAM_GATHER then names the
 // variant.
 int choose_engines(sp_solver *s) {
-    s->sv_p64 = SV_LDG8B16;
-    s->sv_p32 = SV_LDG8B16;
+    s->sv_p64 = SV_LDG4_DEEP;
+    s->sv_p32 = SV_LDG4;
     s->sv_d64 = -1;
-    s->sv_d32 = SV_CP4;
+    s->sv_d32 = SV_LDG8B16;
     const char *eng = getenv("SP_PASS_ENGINE");
     if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
     if (eng && !strcmp(eng, "stream")) {
-        int v = SV_LDG8;
+        int v = SV_LDG4;
         const char *gv = getenv("SP_STREAM_GATHER");
-        const char *names[SV_COUNT] = {"ldg4", "ldg8", "ldg8b16", "ldg12", "cp4"};
+        const char *names[SV_COUNT] = {"ldg4", "ldg4deep", "ldg8b16", "ldg8b16deep", "cp4"};
         for (int k = 0; gv && k < SV_COUNT; ++k)
             if (!strcmp(gv, names[k])) v = k;
         s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = v;

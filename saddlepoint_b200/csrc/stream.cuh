@@ -113,13 +113,17 @@ constexpr int stream_threads(int gw) { return NT + 32 + 32 * gw; }
 
 // Shared memory of one op: S slots of [column indices | values | row pointers |
 // gathered entries | row schedule | row inputs], scratch of the long-row tree, 3·S
-// mbarriers, the abort flag. FP64 ops take 3 slots (190 KB for the primal pass),
-// FP32 ops 4.
-template <class Op>
+// mbarriers, the abort flag. Register gatherers (GREG = false) write each product
+// v·g over its value, so their slots have no gathered-entry region. DEEP: as many
+// slots as fit in the 227 KB a CTA may have (at most 6); otherwise 3 for FP64 ops
+// and 4 for FP32 ones, which leaves part of the SM's 256 KB of L1/shared memory to
+// the L1 cache that the gathers hit.
+constexpr size_t STREAM_SMEM_MAX = 232448;
+
+template <class Op, bool GREG, bool DEEP>
 struct StreamLayout {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
-    static constexpr int S = sizeof(VT) == 4 ? 4 : 3;
     static constexpr int IA = 16 / (int)sizeof(int);       // int32 elements per 16 bytes
     static constexpr int VA = 16 / (int)sizeof(VT);        // value elements per 16 bytes
     static constexpr int DA = 16 / (int)sizeof(double);    // row-input elements per 16 bytes
@@ -128,7 +132,7 @@ struct StreamLayout {
     static constexpr size_t ci_bytes = up16(sizeof(int) * (TILE_NNZ + 2 * IA));
     static constexpr size_t v_bytes = up16(sizeof(VT) * (TILE_NNZ + 2 * VA));
     static constexpr size_t rp_bytes = up16(sizeof(int) * (TILE_ROWS + 1 + 2 * IA));
-    static constexpr size_t g_bytes = up16(sizeof(GT) * TILE_NNZ);
+    static constexpr size_t g_bytes = GREG ? up16(sizeof(GT) * TILE_NNZ) : 0;
     static constexpr size_t sch_bytes = up16(sizeof(uint16_t) * (TILE_ROWS + 2 * SA));
     static constexpr int PRE_STRIDE = TILE_ROWS + 2 * DA;  // doubles per row-input array
     static constexpr size_t pre_bytes = sizeof(double) * PRE_STRIDE * Op::NPRE;
@@ -139,12 +143,25 @@ struct StreamLayout {
     static constexpr size_t sch_off = g_off + g_bytes;
     static constexpr size_t pre_off = sch_off + sch_bytes;
     static constexpr size_t slot = pre_off + pre_bytes;
+    static constexpr size_t fixed = sizeof(double) * (NT / 32) + 3 * 6 * sizeof(unsigned long long) + 16;
+    static constexpr int S_FIT = (int)((STREAM_SMEM_MAX - fixed) / slot) < 6 ? (int)((STREAM_SMEM_MAX - fixed) / slot) : 6;
+    static constexpr int S = DEEP ? S_FIT : (sizeof(VT) == 4 ? 4 : 3);
+    static_assert(S >= 2, "at least two slots");
     static constexpr size_t red_off = S * slot;
     static constexpr size_t bar_off = red_off + sizeof(double) * (NT / 32);
-    static constexpr size_t flag_off = bar_off + 3 * S * sizeof(unsigned long long);
+    static constexpr size_t flag_off = bar_off + 3 * 6 * sizeof(unsigned long long);
     static constexpr size_t total = flag_off + 16;
     static_assert(slot % 16 == 0 && (PRE_STRIDE * sizeof(double)) % 16 == 0, "16-byte aligned regions");
 };
+
+// Product x of a staged tile: already in place of the value (register gatherers), or
+// formed from the value and the gathered entry (cp.async gatherers).
+template <bool IN_PLACE, class Op>
+__device__ __forceinline__ typename Op::ST prod_at(const Op &op, const typename Op::VT *vs, const typename Op::GT *gs,
+                                                   int x) {
+    if constexpr (IN_PLACE) return reinterpret_cast<const typename Op::ST *>(vs)[x];
+    else return op.mul(vs[x], gs[x]);
+}
 
 template <class Op>
 __device__ __forceinline__ void stream_abort(const Op &op, int *abort) {
@@ -210,14 +227,17 @@ __device__ __forceinline__ void consumer_long_row(Op &op, double *sh, int tile) 
 }
 
 // GW gatherer warps; LDG: gathers through registers (B loads in flight per lane,
-// then shared stores and a plain arrive) instead of cp.async.
-template <int GW, bool LDG, int B, class Op>
+// then the products stored over the values and a plain arrive) instead of cp.async;
+// DEEP: the slot count (StreamLayout).
+template <int GW, bool LDG, int B, bool DEEP, class Op>
 __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntiles, int nlong) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
-    using L = StreamLayout<Op>;
+    using ST = typename Op::ST;
+    using L = StreamLayout<Op, !LDG, DEEP>;
     constexpr int S = L::S;
     static_assert(Op::G == 1 && Op::NP == 0, "the stream engine runs passes that gather one vector and reduce nothing");
+    static_assert(!LDG || sizeof(ST) == sizeof(VT), "a product takes its value's place");
     constexpr bool F32 = (Op::F32 & 1u) != 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *bar_load = reinterpret_cast<unsigned long long *>(smem + L::bar_off);
@@ -292,6 +312,8 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
             const int *cs = reinterpret_cast<const int *>(slot + L::ci_off) + (t.z & (L::IA - 1));
             GT *gs = reinterpret_cast<GT *>(smem + s * L::slot + L::g_off);
             if constexpr (LDG) {
+                // the product v·g replaces the staged value (one shared array for the sums)
+                ST *ps = reinterpret_cast<ST *>(smem + s * L::slot + L::v_off) + (t.z & (L::VA - 1));
                 constexpr int W = 32 * GW;
                 for (int base = g * 32 + lane; base < nk; base += W * B) {
                     GT v[B];
@@ -300,7 +322,10 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
                         if (base + u * W < nk) v[u] = __ldg(gv + cs[base + u * W]);
 #pragma unroll
                     for (int u = 0; u < B; ++u)
-                        if (base + u * W < nk) gs[base + u * W] = v[u];
+                        if (base + u * W < nk) {
+                            const int e = base + u * W;
+                            ps[e] = op.mul(reinterpret_cast<const VT *>(ps)[e], v[u]);
+                        }
                 }
                 mbar_arrive(bar_gath + s);  // release: the stores above are visible to the waiters
             } else {
@@ -346,11 +371,11 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
             double sum[1];
             if constexpr (F32) {
                 float f = -0.0f;
-                for (int x = a; x < b; ++x) f += float(op.mul(vs[x], gs[x]));
+                for (int x = a; x < b; ++x) f += float(prod_at<LDG>(op, vs, gs, x));
                 sum[0] = double(f);
             } else {
                 double d = -0.0;
-                for (int x = a; x < b; ++x) d += double(op.mul(vs[x], gs[x]));
+                for (int x = a; x < b; ++x) d += double(prod_at<LDG>(op, vs, gs, x));
                 sum[0] = d;
             }
             op.row(r0 + q, sum, part, op.pre_smem(pres + q, L::PRE_STRIDE));
@@ -363,11 +388,11 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
             double sum[1];
             if constexpr (F32) {
                 float f = -0.0f;
-                for (int x = a + lane; x < b; x += 32) f += float(op.mul(vs[x], gs[x]));
+                for (int x = a + lane; x < b; x += 32) f += float(prod_at<LDG>(op, vs, gs, x));
                 sum[0] = double(warp_sum_down(f));
             } else {
                 double d = -0.0;
-                for (int x = a + lane; x < b; x += 32) d += double(op.mul(vs[x], gs[x]));
+                for (int x = a + lane; x < b; x += 32) d += double(prod_at<LDG>(op, vs, gs, x));
                 sum[0] = warp_sum_down(d);
             }
             if (lane == 0) op.row(r0 + q, sum, part, op.pre_smem(pres + q, L::PRE_STRIDE));
@@ -379,11 +404,11 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
 
 // Runs the pass `op` if its setup() accepts this launch (a uniform choice: it
 // depends only on the device state). One CTA of stream_threads(GW) per SM, with
-// StreamLayout<Op>::total bytes of dynamic shared memory.
-template <class Op, int GW, bool LDG, int B>
+// StreamLayout<Op, !LDG, DEEP>::total bytes of dynamic shared memory.
+template <class Op, int GW, bool LDG, int B, bool DEEP>
 __global__ void __launch_bounds__(stream_threads(GW), 1) k_stream(int ntiles, int nlong, Op op) {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (op.setup()) stream_run<GW, LDG, B>(op, smem, ntiles, nlong);
+    if (op.setup()) stream_run<GW, LDG, B, DEEP>(op, smem, ntiles, nlong);
 }
 
 }  // namespace sp

@@ -17,7 +17,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = ["ldg4", "ldg8", "ldg8b16", "ldg12", "cp4"]
+VARIANTS = ["ldg4", "ldg4deep", "ldg8b16", "ldg8b16deep", "cp4"]
 
 
 def sp():
@@ -26,7 +26,7 @@ def sp():
     return saddlepoint_b200
 
 
-def solve_with(engine, lp, params, backend, variant="ldg8"):
+def solve_with(engine, lp, params, backend, variant="ldg4"):
     old = {k: os.environ.get(k) for k in ("SP_PASS_ENGINE", "SP_STREAM_GATHER")}
     os.environ["SP_PASS_ENGINE"] = engine
     os.environ["SP_STREAM_GATHER"] = variant
@@ -109,7 +109,7 @@ def test_stream_engine_mixed_form_equals_tile_engine(powerlaw_lp, gpu_backend):
 def test_stream_engine_long_rows_and_empty_tiles(gpu_backend):
     lp = ragged_lp()
     params = fixed_iterations(256)
-    for variant in ("ldg8", "cp4"):
+    for variant in ("ldg4deep", "cp4"):
         assert_identical(solve_with("stream", lp, params, gpu_backend, variant),
                          solve_with("tiles", lp, params, gpu_backend))
 
