@@ -519,7 +519,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
         if ((rc = balloc(b, p, no))) return bail(rc, "out of device memory");
     for (double **p : mvecs)
         if ((rc = balloc(b, p, mo))) return bail(rc, "out of device memory");
-    if ((rc = balloc(b, &A.pk, no))) return bail(rc, "out of device memory");
+    if ((rc = balloc(b, &A.pk, no)) || (rc = balloc(b, &A.pky, mo))) return bail(rc, "out of device memory");
     A.a_v32 = A.t_v32 = nullptr;
     A.xbar32 = A.y32 = nullptr;
     if (b->mixed) {

@@ -54,6 +54,7 @@ struct BatchArgs {
     double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty, *pv, *pt, *ox, *oy;
     float *xbar32, *y32;
     CheckQuad *pk;  // the tile variant's packed column records (n per instance)
+    double2 *pky;   // ... and row records (m per instance)
     const Tile *a_tiles, *t_tiles;
     double *part;  // per-tile partial sums of every instance
     sp_batch_result *res;
@@ -500,6 +501,7 @@ __device__ void batch_solve_one(const BatchArgs &A, int id, double *sh, DevState
         S.xbar32 = xbar32;
         S.y32 = y32;
         S.pk = A.pk + I.no;
+        S.pky = A.pky + I.mo;
         double *pt_base = A.part + I.pt, *pa_base = A.part + I.pa;
         S.partP = pt_base;
         S.partT = pt_base + (long long)I.ntt * NP_P;

@@ -188,7 +188,7 @@ extern "C" int64_t sp_server_footprint(int64_t m, int64_t n, int64_t nnz, int pr
     // n- and m-vectors of the solve, and 8 MiB of fixed overhead.
     int64_t b = 2 * nnz * 12 + 24 * nnz + 4 * (m + n + 2);
     if (precision == SP_PRECISION_MIXED) b += 2 * nnz * 4 + 4 * (m + n);
-    b += 168 * n + 104 * m + (8ll << 20);
+    b += 168 * n + 120 * m + (8ll << 20);
     return b;
 }
 

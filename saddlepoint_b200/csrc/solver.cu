@@ -424,6 +424,7 @@ SolverPtrs ptrs_of(sp_solver *s) {
     p.xbar32 = s->xbar32;
     p.y32 = s->y32;
     p.pk = s->pk;
+    p.pky = s->pky;
     p.partP = s->partP;
     p.partD = s->partD;
     p.partT = s->partT;
@@ -467,21 +468,31 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
 // The stream engine kernels of one FUSED op: one CTA per SM. Variants differ in the
 // gatherer warps (count, loads in flight per lane, register or cp.async gathers) and
 // in the slot count; choose_engines() picks one per pass when a solver is created.
-enum StreamVariant : int { SV_LDG4 = 0, SV_LDG4_DEEP, SV_LDG8B16, SV_LDG8B16_DEEP, SV_CP4, SV_COUNT };
+enum StreamVariant : int {
+    SV_LDG4 = 0,    // 4 register-gatherer warps, 8 loads in flight per lane
+    SV_LDG4_DEEP,   // ... with as many slots as fit
+    SV_LDG8B16,     // 8 warps, 16 loads in flight per lane
+    SV_CP4,         // 4 cp.async gatherer warps
+    SV_LDG4_G2,     // SV_LDG4 with two consumer groups
+    SV_LDG4_DEEP_G2,
+    SV_LDG8B16_G2,
+    SV_COUNT
+};
+constexpr const char *STREAM_VARIANT_NAMES[SV_COUNT] = {"ldg4",   "ldg4deep",   "ldg8b16",  "cp4",
+                                                        "ldg4g2", "ldg4deepg2", "ldg8b16g2"};
 
 template <class Op>
 struct StreamKernel {
     template <bool LDG, bool DEEP>
     static constexpr size_t smem_of() { return StreamLayout<Op, !LDG, DEEP>::total; }
     static std::atomic<int> ready[64];
-    template <int GW, bool LDG, int B, bool DEEP>
+    template <int GW, bool LDG, int B, bool DEEP, int CG>
     static int prepare_one() {
         constexpr size_t smem = smem_of<LDG, DEEP>();
-        SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_stream<Op, GW, LDG, B, DEEP>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        auto *f = k_stream<Op, GW, LDG, B, DEEP, CG>;
+        SP_CUDA_TRY(cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int b = 0;
-        SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_stream<Op, GW, LDG, B, DEEP>,
-                                                                  stream_threads(GW), smem));
+        SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, stream_threads(GW), smem));
         if (b < 1) return fail(SP_ERR_CUDA, "stream engine kernel cannot be resident");
         return SP_OK;
     }
@@ -490,25 +501,29 @@ struct StreamKernel {
         if (dev < 0 || dev >= 64) return fail(SP_ERR_INVALID, "device ordinal out of range");
         if (ready[dev].load()) return SP_OK;
         int rc;
-        if ((rc = prepare_one<4, true, 8, false>()) || (rc = prepare_one<4, true, 8, true>()) ||
-            (rc = prepare_one<8, true, 16, false>()) || (rc = prepare_one<8, true, 16, true>()) ||
-            (rc = prepare_one<4, false, 1, false>()))
+        if ((rc = prepare_one<4, true, 8, false, 1>()) || (rc = prepare_one<4, true, 8, true, 1>()) ||
+            (rc = prepare_one<8, true, 16, false, 1>()) || (rc = prepare_one<4, false, 1, false, 1>()) ||
+            (rc = prepare_one<4, true, 8, false, 2>()) || (rc = prepare_one<4, true, 8, true, 2>()) ||
+            (rc = prepare_one<8, true, 16, false, 2>()))
             return rc;
         ready[dev].store(1);
         return SP_OK;
     }
-    template <int GW, bool LDG, int B, bool DEEP>
+    template <int GW, bool LDG, int B, bool DEEP, int CG>
     static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op) {
-        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op);
+        k_stream<Op, GW, LDG, B, DEEP, CG><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong,
+                                                                                                   op);
     }
     static void launch(const sp_ctx *ctx, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctx->sms, M.ntiles));
         switch (variant) {
-        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op); break;
-        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op); break;
-        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op); break;
-        case SV_LDG8B16_DEEP: go<8, true, 16, true>(grid, M, st, op); break;
-        default: go<4, false, 1, false>(grid, M, st, op); break;
+        case SV_LDG4: go<4, true, 8, false, 1>(grid, M, st, op); break;
+        case SV_LDG4_DEEP: go<4, true, 8, true, 1>(grid, M, st, op); break;
+        case SV_LDG8B16: go<8, true, 16, false, 1>(grid, M, st, op); break;
+        case SV_LDG4_G2: go<4, true, 8, false, 2>(grid, M, st, op); break;
+        case SV_LDG4_DEEP_G2: go<4, true, 8, true, 2>(grid, M, st, op); break;
+        case SV_LDG8B16_G2: go<8, true, 16, false, 2>(grid, M, st, op); break;
+        default: go<4, false, 1, false, 1>(grid, M, st, op); break;
         }
     }
 };
@@ -538,9 +553,8 @@ int choose_engines(sp_solver *s) {
     if (eng && !strcmp(eng, "stream")) {
         int v = SV_LDG4;
         const char *gv = getenv("SP_STREAM_GATHER");
-        const char *names[SV_COUNT] = {"ldg4", "ldg4deep", "ldg8b16", "ldg8b16deep", "cp4"};
         for (int k = 0; gv && k < SV_COUNT; ++k)
-            if (!strcmp(gv, names[k])) v = k;
+            if (!strcmp(gv, STREAM_VARIANT_NAMES[k])) v = k;
         s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = v;
     }
     const int dev = s->ctx->device;
@@ -716,7 +730,7 @@ void solver_release(sp_solver *s) {
     free_csr(&s->A, fst);
     free_csr(&s->AT, fst);
     void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
-                    s->aty, s->xbar32, s->y32, s->pk, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
+                    s->aty, s->xbar32, s->y32, s->pk, s->pky, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
                     s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,
                     s->out_x, s->out_y};
     for (void *b : bufs) dfree(b, fst);
@@ -1008,7 +1022,7 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     if ((rc = dalloc(&s->x, n)) || (rc = dalloc(&s->y, m)) || (rc = dalloc(&s->xt, n)) || (rc = dalloc(&s->yt, m)) ||
         (rc = dalloc(&s->xbar, n)) || (rc = dalloc(&s->xa, n)) || (rc = dalloc(&s->ya, m)) ||
         (rc = dalloc(&s->aty, n)) || (rc = dalloc(&s->xbar32, n)) || (rc = dalloc(&s->y32, m)) ||
-        (rc = dalloc(&s->pk, n)) ||
+        (rc = dalloc(&s->pk, n)) || (rc = dalloc(&s->pky, m)) ||
         (rc = dalloc(&s->partP, (int64_t)s->AT.ntiles * NP_P)) || (rc = dalloc(&s->partT, (int64_t)s->AT.ntiles * NP_T)) ||
         (rc = dalloc(&s->partP0, (int64_t)s->AT.ntiles * NP_P0)) ||
         (rc = dalloc(&s->partD, (int64_t)s->A.ntiles * NP_D)) || (rc = dalloc(&s->partD0, (int64_t)s->A.ntiles * NP_D0)) ||

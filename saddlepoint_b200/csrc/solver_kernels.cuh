@@ -48,6 +48,7 @@ struct SolverPtrs {
     double *x, *y, *xt, *yt, *xbar, *xa, *ya, *aty;
     float *xbar32, *y32;
     CheckQuad *pk;
+    double2 *pky;  // the check's dual records for T: y_t, y_t - y_anchor (16 bytes per row)
     // partial sums per tile
     double *partP, *partD, *partT, *partP0, *partD0;
     const DevParams *prm;
@@ -271,6 +272,7 @@ struct DualPass {
                 const double lc = in.lc, uc = in.uc;
                 const double e = excess(sum[2], lc, uc) * in.pf;
                 const double dya = yt - in.ya;
+                s.pky[r] = make_double2(yt, dya);
                 const double rv = recession_violation(sum[3], lc, uc);
                 const double fb = forbidden(dya, lc, uc);
                 part[2] += e * e;                       // primal residual
@@ -310,9 +312,9 @@ struct CheckPassT {
         return true;
     }
     __device__ __forceinline__ void prod(int c, double v, double (&p)[2]) const {
-        const double ytc = __ldg(s.yt + c);
-        p[0] = v * ytc;
-        p[1] = v * (ytc - __ldg(s.ya + c));
+        const double2 q = __ldg(s.pky + c);  // y_t and y_t - y_anchor, one sector
+        p[0] = v * q.x;
+        p[1] = v * q.y;
     }
     struct Pre {
         double lv, uv, df, c, aty, xt, x;

@@ -34,6 +34,7 @@ struct sp_solver {
            *aty = nullptr;
     float *xbar32 = nullptr, *y32 = nullptr;
     sp::CheckQuad *pk = nullptr;  // the check's packed column records
+    double2 *pky = nullptr;       // ... and row records
     // partial sums per tile
     double *partP = nullptr, *partD = nullptr, *partT = nullptr, *partP0 = nullptr, *partD0 = nullptr;
     // power iteration
