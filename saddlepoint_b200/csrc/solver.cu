@@ -469,27 +469,23 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
 // gatherer warps (count, loads in flight per lane, register or cp.async gathers) and
 // in the slot count; choose_engines() picks one per pass when a solver is created.
 enum StreamVariant : int {
-    SV_LDG4 = 0,    // 4 register-gatherer warps, 8 loads in flight per lane
-    SV_LDG4_DEEP,   // ... with as many slots as fit
-    SV_LDG8B16,     // 8 warps, 16 loads in flight per lane
-    SV_CP4,         // 4 cp.async gatherer warps
-    SV_LDG4_G2,     // SV_LDG4 with two consumer groups
-    SV_LDG4_DEEP_G2,
-    SV_LDG8B16_G2,
+    SV_LDG4 = 0,   // 4 register-gatherer warps, 8 loads in flight per lane
+    SV_LDG4_DEEP,  // ... with as many slots as fit
+    SV_LDG8B16,    // 8 warps, 16 loads in flight per lane
+    SV_CP4,        // 4 cp.async gatherer warps
     SV_COUNT
 };
-constexpr const char *STREAM_VARIANT_NAMES[SV_COUNT] = {"ldg4",   "ldg4deep",   "ldg8b16",  "cp4",
-                                                        "ldg4g2", "ldg4deepg2", "ldg8b16g2"};
+constexpr const char *STREAM_VARIANT_NAMES[SV_COUNT] = {"ldg4", "ldg4deep", "ldg8b16", "cp4"};
 
 template <class Op>
 struct StreamKernel {
     template <bool LDG, bool DEEP>
     static constexpr size_t smem_of() { return StreamLayout<Op, !LDG, DEEP>::total; }
     static std::atomic<int> ready[64];
-    template <int GW, bool LDG, int B, bool DEEP, int CG>
+    template <int GW, bool LDG, int B, bool DEEP>
     static int prepare_one() {
         constexpr size_t smem = smem_of<LDG, DEEP>();
-        auto *f = k_stream<Op, GW, LDG, B, DEEP, CG>;
+        auto *f = k_stream<Op, GW, LDG, B, DEEP>;
         SP_CUDA_TRY(cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int b = 0;
         SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, stream_threads(GW), smem));
@@ -501,29 +497,23 @@ struct StreamKernel {
         if (dev < 0 || dev >= 64) return fail(SP_ERR_INVALID, "device ordinal out of range");
         if (ready[dev].load()) return SP_OK;
         int rc;
-        if ((rc = prepare_one<4, true, 8, false, 1>()) || (rc = prepare_one<4, true, 8, true, 1>()) ||
-            (rc = prepare_one<8, true, 16, false, 1>()) || (rc = prepare_one<4, false, 1, false, 1>()) ||
-            (rc = prepare_one<4, true, 8, false, 2>()) || (rc = prepare_one<4, true, 8, true, 2>()) ||
-            (rc = prepare_one<8, true, 16, false, 2>()))
+        if ((rc = prepare_one<4, true, 8, false>()) || (rc = prepare_one<4, true, 8, true>()) ||
+            (rc = prepare_one<8, true, 16, false>()) || (rc = prepare_one<4, false, 1, false>()))
             return rc;
         ready[dev].store(1);
         return SP_OK;
     }
-    template <int GW, bool LDG, int B, bool DEEP, int CG>
+    template <int GW, bool LDG, int B, bool DEEP>
     static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op) {
-        k_stream<Op, GW, LDG, B, DEEP, CG><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong,
-                                                                                                   op);
+        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op);
     }
     static void launch(const sp_ctx *ctx, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctx->sms, M.ntiles));
         switch (variant) {
-        case SV_LDG4: go<4, true, 8, false, 1>(grid, M, st, op); break;
-        case SV_LDG4_DEEP: go<4, true, 8, true, 1>(grid, M, st, op); break;
-        case SV_LDG8B16: go<8, true, 16, false, 1>(grid, M, st, op); break;
-        case SV_LDG4_G2: go<4, true, 8, false, 2>(grid, M, st, op); break;
-        case SV_LDG4_DEEP_G2: go<4, true, 8, true, 2>(grid, M, st, op); break;
-        case SV_LDG8B16_G2: go<8, true, 16, false, 2>(grid, M, st, op); break;
-        default: go<4, false, 1, false, 1>(grid, M, st, op); break;
+        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op); break;
+        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op); break;
+        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op); break;
+        default: go<4, false, 1, false>(grid, M, st, op); break;
         }
     }
 };

@@ -228,9 +228,8 @@ __device__ __forceinline__ void consumer_long_row(Op &op, double *sh, int tile) 
 
 // GW gatherer warps; LDG: gathers through registers (B loads in flight per lane,
 // then the products stored over the values and a plain arrive) instead of cp.async;
-// DEEP: the slot count (StreamLayout); CG: consumer groups — the eight consumer warps
-// split into CG groups that take alternate tiles, so CG tiles are summed at once.
-template <int GW, bool LDG, int B, bool DEEP, int CG, class Op>
+// DEEP: the slot count (StreamLayout).
+template <int GW, bool LDG, int B, bool DEEP, class Op>
 __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntiles, int nlong) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
@@ -253,7 +252,7 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
         for (int s = 0; s < S; ++s) {
             mbar_init(bar_load + s, 1);
             mbar_init(bar_gath + s, 32 * GW);
-            mbar_init(bar_empty + s, STREAM_CONSUMER_WARPS / CG);
+            mbar_init(bar_empty + s, STREAM_CONSUMER_WARPS);
         }
         *abort = 0;
         mbar_init_fence();
@@ -344,11 +343,8 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
         consumer_long_row(op, reinterpret_cast<double *>(smem + L::red_off), t);
         consumer_sync();
     }
-    constexpr int CW = STREAM_CONSUMER_WARPS / CG, NTG = 32 * CW;  // warps and threads per group
-    static_assert(CW * CG == STREAM_CONSUMER_WARPS && (CW & (CW - 1)) == 0, "groups of a power-of-two warps");
-    const int grp = warp / CW, gwarp = warp % CW, gtid = tid % NTG;
     double part[1] = {0.0};
-    for (int j = grp; j < nmine; j += CG) {
+    for (int j = 0; j < nmine; ++j) {
         const int s = j % S, k = j / S;
         if (!stream_wait(bar_load + s, (unsigned)k & 1u, abort_v) ||
             !stream_wait(bar_gath + s, (unsigned)k & 1u, abort_v)) {
@@ -363,11 +359,11 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
         const GT *gs = reinterpret_cast<const GT *>(slot + L::g_off);
         const uint16_t *ss = reinterpret_cast<const uint16_t *>(slot + L::sch_off) + (r0 & (L::SA - 1));
         const double *pres = reinterpret_cast<const double *>(slot + L::pre_off) + (r0 & (L::DA - 1));
-        // Schedule slots are dealt to the group's threads (and the flagged tail to its
-        // warps) with an offset that rotates per tile by whole warps, so short tiles do
-        // not always land on the same warps.
-        const int rot = (j / CG) & (CW - 1);
-        for (int u = (gtid + 32 * rot) & (NTG - 1); u < nr; u += NTG) {
+        // Schedule slots are dealt to threads (and the flagged tail to warps) with an
+        // offset that rotates per tile by whole warps, so short tiles do not always
+        // land on the same warps.
+        const int rot = j & 7;
+        for (int u = (tid + 32 * rot) & (NT - 1); u < nr; u += NT) {
             const int e = ss[u];
             if (e & SCHED_WARP) continue;
             const int q = e;
@@ -384,7 +380,7 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
             }
             op.row(r0 + q, sum, part, op.pre_smem(pres + q, L::PRE_STRIDE));
         }
-        for (int u = nr - 1 - ((gwarp + rot) & (CW - 1)); u >= 0; u -= CW) {
+        for (int u = nr - 1 - ((warp + rot) & 7); u >= 0; u -= NT / 32) {
             const int e = ss[u];
             if (!(e & SCHED_WARP)) break;
             const int q = e & (SCHED_WARP - 1);
@@ -409,10 +405,10 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
 // Runs the pass `op` if its setup() accepts this launch (a uniform choice: it
 // depends only on the device state). One CTA of stream_threads(GW) per SM, with
 // StreamLayout<Op, !LDG, DEEP>::total bytes of dynamic shared memory.
-template <class Op, int GW, bool LDG, int B, bool DEEP, int CG>
+template <class Op, int GW, bool LDG, int B, bool DEEP>
 __global__ void __launch_bounds__(stream_threads(GW), 1) k_stream(int ntiles, int nlong, Op op) {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (op.setup()) stream_run<GW, LDG, B, DEEP, CG>(op, smem, ntiles, nlong);
+    if (op.setup()) stream_run<GW, LDG, B, DEEP>(op, smem, ntiles, nlong);
 }
 
 }  // namespace sp

@@ -17,7 +17,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = ["ldg4", "ldg4deep", "ldg8b16", "cp4", "ldg4g2", "ldg4deepg2", "ldg8b16g2"]
+VARIANTS = ["ldg4", "ldg4deep", "ldg8b16", "cp4"]
 
 
 def sp():
@@ -109,7 +109,7 @@ def test_stream_engine_mixed_form_equals_tile_engine(powerlaw_lp, gpu_backend):
 def test_stream_engine_long_rows_and_empty_tiles(gpu_backend):
     lp = ragged_lp()
     params = fixed_iterations(256)
-    for variant in ("ldg4deep", "cp4", "ldg8b16g2"):
+    for variant in ("ldg4deep", "cp4"):
         assert_identical(solve_with("stream", lp, params, gpu_backend, variant),
                          solve_with("tiles", lp, params, gpu_backend))
 
