@@ -323,7 +323,7 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded generator, see DESIGN.md)",
+        "data": "synthetic (seeded generators of saddlepoint_b200/csrc/host.cpp)",
         "config": dict(WORKLOAD_DESC[args.workload], parallelism=f"replicas x{n}", seed=args.seed,
                        **({"scale": args.scale, "m": lp.nrows, "n": lp.ncols, "nnz": lp.nnz} if args.scale != 1.0 else {})),
         "roofline": roofline(f64),
@@ -393,7 +393,7 @@ def run_reference(args):
         "impl": "reference", "metric": "PDHG iter/s (FP64, device-resident)", "value": value, "unit": "iter/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded generator, see DESIGN.md)",
+        "data": "synthetic (seeded generators of saddlepoint_b200/csrc/host.cpp)",
         "config": dict(WORKLOAD_DESC["powerlaw"], parallelism="host threads", seed=args.seed),
         "cpu_baseline": {"value": value, "unit": "iter/s", "cores": oracle.get_threads(), "kind": "port",
                          "sample": sample},

@@ -42,6 +42,7 @@ extern "C" {
 #define SP_ERR_NUMERICAL 5   /* SolveError::Numerical */
 #define SP_ERR_PROBLEM 6     /* SolveError::Problem: LpProblem::validate failed */
 #define SP_ERR_DEVICE 7      /* a kernel reported an error (e.g. a bounded wait ran out) */
+#define SP_ERR_PARSE 8       /* MpsError::Parse: malformed MPS text (line and message returned) */
 
 /* ---- Status (crates/saddlepoint-core/src/solver.rs:95-102) ---- */
 #define SP_STATUS_OPTIMAL 0
@@ -313,7 +314,7 @@ void sp_server_destroy(sp_server *s);
 int sp_dot_noalloc(const double *a, const double *b, int64_t n, double *result, void *stream);
 
 /* ========================================================================
- * Synthetic LP generators (seeded; see DESIGN.md for the exact recipes).
+ * Synthetic LP generators (seeded; the recipes are in csrc/host.cpp).
  * ======================================================================== */
 
 #define SP_GEN_RANDOM 0    /* random sparse LP: config-0 style */
@@ -334,6 +335,17 @@ typedef struct {
 /* Generated LP with library-owned host arrays; release with sp_lp_release. */
 int sp_generate(const sp_gen_params *g, sp_lp *out);
 void sp_lp_release(sp_lp *lp);
+
+/* ========================================================================
+ * Part 5 — problem input.
+ * ======================================================================== */
+
+/* read_mps (crates/saddlepoint-io/src/lib.rs:59-309): free-format MPS text of `len`
+ * bytes to an LP with library-owned host arrays (release with sp_lp_release), the
+ * matrix built as CsrMatrix::from_triplets builds it (problem.rs:33-77). On malformed
+ * text returns SP_ERR_PARSE with the 1-based line in *err_line and the reference's
+ * message in err (any of the two may be null). Row and column names are not kept. */
+int sp_read_mps(const char *text, size_t len, sp_lp *out, int64_t *err_line, char *err, size_t errlen);
 
 #ifdef __cplusplus
 }

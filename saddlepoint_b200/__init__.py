@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -30,7 +31,7 @@ from . import _lib as L
 __all__ = [
     "BackendError", "SolveError", "Status", "Termination", "Precision", "LpProblem", "ScaledProblem",
     "SolverParams", "Solution", "CudaBackend", "Solver", "solve", "solve_stepwise", "BatchSolver", "Server",
-    "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library",
+    "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library", "read_mps", "MpsError",
 ]
 
 
@@ -543,6 +544,44 @@ def solve_stepwise(problem, params: Optional[SolverParams] = None, backend: Opti
     return _solution(info, x, y)
 
 
+# ------------------------------------------------------------------ problem input
+
+class MpsError(ValueError):
+    """MpsError::Parse (crates/saddlepoint-io/src/lib.rs:21-27): 'line N: message'."""
+
+    def __init__(self, line: int, msg: str):
+        super().__init__(f"line {line}: {msg}")
+        self.line, self.msg = line, msg
+
+
+def read_mps(source, name: str = "") -> LpProblem:
+    """read_mps / read_mps_file (crates/saddlepoint-io/src/lib.rs:50-309): MPS text (bytes or
+    str) or a path to a .mps file (.mps.gz is decompressed first) to an LpProblem."""
+    import gzip
+
+    if isinstance(source, (bytes, bytearray)):
+        text = bytes(source)
+    elif isinstance(source, str) and ("\n" in source or not os.path.exists(source)):
+        text = source.encode()
+    else:
+        path = os.fspath(source)
+        with open(path, "rb") as fh:
+            text = fh.read()
+        if path.endswith(".gz"):
+            text = gzip.decompress(text)
+        name = name or os.path.basename(path).split(".")[0]
+    lib = library()
+    out = L.Lp()
+    line = L.i64(0)
+    err = C.create_string_buffer(256)
+    rc = lib.sp_read_mps(text, len(text), C.byref(out), C.byref(line), err, 256)
+    if rc == L.SP_ERR_PARSE:
+        raise MpsError(int(line.value), err.value.decode())
+    if rc != L.SP_OK:
+        raise BackendError(rc, "sp_read_mps failed")
+    return _take_lp(out, name)
+
+
 # ------------------------------------------------------------------ generators
 
 def _generate(gp: L.GenParams, name: str) -> LpProblem:
@@ -551,6 +590,12 @@ def _generate(gp: L.GenParams, name: str) -> LpProblem:
     rc = lib.sp_generate(C.byref(gp), C.byref(out))
     if rc != L.SP_OK:
         raise BackendError(rc, "generator rejected its parameters")
+    return _take_lp(out, name)
+
+
+def _take_lp(out: L.Lp, name: str) -> LpProblem:
+    """Copies a library-owned sp_lp into an LpProblem and releases it."""
+    lib = library()
     m, n, nnz = out.a.nrows, out.a.ncols, out.a.nnz
 
     def arr(ptr, k, dt):

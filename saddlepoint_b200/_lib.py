@@ -20,6 +20,7 @@ PI32 = C.POINTER(C.c_int32)
 VP = C.c_void_p
 
 SP_OK = 0
+SP_ERR_PARSE = 8
 ERRORS = {
     1: "CUDA error",
     2: "invalid argument",
@@ -28,6 +29,7 @@ ERRORS = {
     5: "numerical breakdown",
     6: "invalid problem",
     7: "device error",
+    8: "MPS parse error",
 }
 
 
@@ -163,6 +165,7 @@ SIGNATURES = [
     ("sp_dot_noalloc", cint, [VP, VP, i64, VP, VP]),
     ("sp_generate", cint, [C.POINTER(GenParams), C.POINTER(Lp)]),
     ("sp_lp_release", None, [C.POINTER(Lp)]),
+    ("sp_read_mps", cint, [C.c_char_p, C.c_size_t, C.POINTER(Lp), C.POINTER(i64), C.c_char_p, C.c_size_t]),
 ]
 
 _lib = None

@@ -662,6 +662,41 @@ extern "C" int sp_generate(const sp_gen_params *g, sp_lp *out) {
     return SP_OK;
 }
 
+namespace sp {
+// Hands arrays built elsewhere in the library (the MPS reader) to `out`, owned by the
+// library until sp_lp_release.
+void register_owned_lp(sp_lp *out, std::vector<int64_t> &&rp, std::vector<int32_t> &&ci, std::vector<double> &&v,
+                       std::vector<double> &&c, std::vector<double> &&lc, std::vector<double> &&uc,
+                       std::vector<double> &&lv, std::vector<double> &&uv) {
+    auto *o = new Owned();
+    o->rp = std::move(rp);
+    o->ci = std::move(ci);
+    o->v = std::move(v);
+    o->c = std::move(c);
+    o->lc = std::move(lc);
+    o->uc = std::move(uc);
+    o->lv = std::move(lv);
+    o->uv = std::move(uv);
+    // keep every pointer valid for empty problems
+    for (auto *vec : {&o->v, &o->c, &o->lc, &o->uc, &o->lv, &o->uv}) vec->reserve(1);
+    o->ci.reserve(1);
+    memset(out, 0, sizeof *out);
+    out->a.nrows = (int64_t)o->rp.size() - 1;
+    out->a.ncols = (int64_t)o->c.size();
+    out->a.nnz = (int64_t)o->v.size();
+    out->a.row_ptr = o->rp.data();
+    out->a.col_idx = o->ci.data();
+    out->a.values = o->v.data();
+    out->c = o->c.data();
+    out->lc = o->lc.data();
+    out->uc = o->uc.data();
+    out->lv = o->lv.data();
+    out->uv = o->uv.data();
+    std::lock_guard<std::mutex> lock(g_owned_mu);
+    g_owned[out->a.row_ptr] = o;
+}
+}  // namespace sp
+
 extern "C" void sp_lp_release(sp_lp *lp) {
     if (!lp || !lp->a.row_ptr) return;
     Owned *o = nullptr;
