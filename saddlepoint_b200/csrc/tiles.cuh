@@ -325,8 +325,14 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
                 warp_row(e & (SCHED_WARP - 1));
             }
         } else {
-            for (int i = warp; i < nr; i += NT / 32)
-                if (srp[i + 1] - srp[i] > SEQ_MAX) warp_row(i);
+            // Rows warp, warp + 8, ... in increasing order, as a scan would take them;
+            // a ballot finds the long ones among 32 of them at a time.
+            for (int base = warp; base < nr; base += 32 * (NT / 32)) {
+                const int i = base + lane * (NT / 32);
+                const bool heavy = i < nr && srp[i + 1] - srp[i] > SEQ_MAX;
+                for (unsigned mask = __ballot_sync(0xffffffffu, heavy); mask; mask &= mask - 1)
+                    warp_row(base + (__ffs(mask) - 1) * (NT / 32));
+            }
         }
     }
     if constexpr (NP > 0) {

@@ -180,3 +180,13 @@ def test_mixed_precision_reaches_tolerance(name, gpu_backend):
     if ref.status == "Optimal":
         oracle.check(lp, g.x, g.y).verify(2.0 * TOL)
         assert abs(g.objective - ref.objective) / (1.0 + abs(ref.objective)) <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["afiro", "adlittle", "israel"])
+def test_netlib_read_by_the_library_solves_like_the_oracle(name, gpu_backend):
+    """The product path end to end: sp.read_mps on the fixture file, then sp.solve."""
+    from conftest import NETLIB
+
+    lp = sp().read_mps(f"{NETLIB}/{name}.mps.gz")
+    g = sp().solve(lp, sp().SolverParams(tolerance=TOL), gpu_backend)
+    compare(name, netlib_lp(name), g, reference_solution(name))
