@@ -74,6 +74,7 @@ class Dist:
                 backend = "gloo"
             dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
+            self.device = f"cuda:{self.local}" if backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
@@ -84,7 +85,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
