@@ -6,6 +6,9 @@
 // estimate_norm, kkt, fixed_point_residual, infeasibility, PidState) and
 // crates/saddlepoint-core/src/scaling.rs:53-103 (ScaledProblem::new).
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <atomic>
@@ -468,6 +471,8 @@ DualPass<LO, MODE> mkD(const SolverPtrs &p, int i, int role) {
 // The stream engine kernels of one FUSED op: one CTA per SM. Variants differ in the
 // gatherer warps (count, loads in flight per lane, register or cp.async gathers) and
 // in the slot count; choose_engines() picks one per pass when a solver is created.
+constexpr int ENGINE_SELL = 100;  // a pass on its SELL copy (sell.cuh)
+
 enum StreamVariant : int {
     SV_LDG4 = 0,   // 4 register-gatherer warps, 8 loads in flight per lane
     SV_LDG4_DEEP,  // ... with as many slots as fit
@@ -525,21 +530,82 @@ using StreamP32 = StreamKernel<PrimalPass<true, 0>>;
 using StreamD64 = StreamKernel<DualPass<false, 0>>;
 using StreamD32 = StreamKernel<DualPass<true, 0>>;
 
-// Which engine runs each MID pass (-1: the tile engine, else a stream variant). The
-// defaults are the fastest measured on the 40M power-law LP (ms per launch): FP64
-// primal on the stream engine, 4 register-gatherer warps, 4 slots (0.255; tile engine
-// 0.301); FP64 dual on the tile engine (0.235; stream 0.300); FP32 primal on the
-// stream engine, 4 gatherer warps, 4 slots (0.247; tile 0.285); FP32 dual on the
-// stream engine, 8 gatherer warps x 16 loads in flight (0.222; tile 0.242).
-// SP_PASS_ENGINE=tiles|stream overrides all four; SP_STREAM_GATHER then names the
-// variant.
+// The SELL copy of one matrix (sell.cuh), built on the device from its CSR arrays after
+// scaling. Left unbuilt (ok = false) for a matrix with a row longer than TILE_NNZ.
+int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
+    cudaStream_t st = s->ctx->stream;
+    *S = SellMat{};
+    if (M.nlong > 0 || M.nrows == 0) return SP_OK;
+    const int64_t nrows = M.nrows, nslices = (nrows + 31) / 32;
+    S->nrows = nrows;
+    S->nslices = nslices;
+    int64_t *slots = nullptr;
+    int *flag = nullptr, *nsel = nullptr;
+    void *tmp = nullptr;
+    int rc;
+    if ((rc = dmalloc((void **)&S->len, nslices * 32)) || (rc = dmalloc((void **)&S->slen, sizeof(int) * nslices)) ||
+        (rc = dmalloc((void **)&S->off, sizeof(int64_t) * nslices)) ||
+        (rc = dmalloc((void **)&slots, sizeof(int64_t) * nslices)) || (rc = dmalloc((void **)&flag, sizeof(int) * nrows)) ||
+        (rc = dmalloc((void **)&S->heavy, sizeof(int) * nrows)) || (rc = dmalloc((void **)&nsel, sizeof(int))))
+        return rc;
+    const int g = grid_of(s->ctx, nslices * 32);
+    k_sell_meta<<<g, NT, 0, st>>>(M.rp, nrows, nslices, S->len, S->slen, slots, flag);
+    size_t b1 = 0, b2 = 0;
+    thrust::counting_iterator<int> rows(0);
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, b1, slots, S->off, (int)nslices, st));
+    SP_CUDA_TRY(cub::DeviceSelect::Flagged(nullptr, b2, rows, flag, S->heavy, nsel, (int)nrows, st));
+    if ((rc = dmalloc(&tmp, std::max(b1, b2)))) return rc;
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, b1, slots, S->off, (int)nslices, st));
+    SP_CUDA_TRY(cub::DeviceSelect::Flagged(tmp, b2, rows, flag, S->heavy, nsel, (int)nrows, st));
+    int64_t last[2];
+    int nh = 0;
+    SP_CUDA_TRY(cudaMemcpyAsync(&last[0], S->off + nslices - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaMemcpyAsync(&last[1], slots + nslices - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaMemcpyAsync(&nh, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    S->slots = last[0] + last[1];
+    S->nheavy = nh;
+    if ((rc = dmalloc((void **)&S->ci, sizeof(int) * std::max<int64_t>(S->slots, 1))) ||
+        (rc = dmalloc((void **)&S->v, sizeof(double) * std::max<int64_t>(S->slots, 1))))
+        return rc;
+    if (s->mixed && (rc = dmalloc((void **)&S->v32, sizeof(float) * std::max<int64_t>(S->slots, 1)))) return rc;
+    k_sell_fill<<<g, NT, 0, st>>>(M.rp, M.ci, M.v, nrows, nslices, S->len, S->off, S->ci, S->v, S->v32);
+    SP_CUDA_TRY(cudaGetLastError());
+    for (void *p : {(void *)slots, (void *)flag, (void *)nsel, tmp}) dfree(p, st);
+    S->ok = true;
+    return SP_OK;
+}
+
+void free_sell(SellMat *S, cudaStream_t st) {
+    for (void *p : {(void *)S->ci, (void *)S->v, (void *)S->v32, (void *)S->off, (void *)S->slen, (void *)S->len,
+                    (void *)S->heavy})
+        dfree(p, st);
+    *S = SellMat{};
+}
+
+template <class Op>
+void launch_sell(const SellMat &S, cudaStream_t st, const Op &op) {
+    const SellArgs a{S.ci, S.v, S.v32, S.off, S.slen, S.len, S.heavy, S.nrows, S.nslices, S.nheavy};
+    const int64_t items = S.nheavy + S.nslices;
+    k_sell<Op><<<(unsigned)((items + NT / 32 - 1) / (NT / 32)), NT, 0, st>>>(op, a);
+}
+
+// Which engine runs each MID pass (-1: the tile engine, ENGINE_SELL the SELL path, else a
+// stream-engine variant). The defaults are the fastest measured on the 40M power-law LP (ms
+// per launch): the primal pass on the stream engine with 4 register-gatherer warps, 4 slots
+// in FP64 (0.255; tile engine 0.297, SELL 0.442 — its short rows are too uneven for slices)
+// and 4 in FP32 (0.247); the dual pass on its SELL copy in both precisions
+// (0.199 FP64, 0.208 FP32; tile engine 0.238 and 0.249, stream engine 0.300 and 0.227).
+// SP_PASS_ENGINE=tiles|stream|sell overrides all four; SP_STREAM_GATHER names the
+// stream variant.
 int choose_engines(sp_solver *s) {
     s->sv_p64 = SV_LDG4_DEEP;
     s->sv_p32 = SV_LDG4;
-    s->sv_d64 = -1;
-    s->sv_d32 = SV_LDG8B16;
+    s->sv_d64 = ENGINE_SELL;
+    s->sv_d32 = ENGINE_SELL;
     const char *eng = getenv("SP_PASS_ENGINE");
     if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
+    if (eng && !strcmp(eng, "sell")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = ENGINE_SELL;
     if (eng && !strcmp(eng, "stream")) {
         int v = SV_LDG4;
         const char *gv = getenv("SP_STREAM_GATHER");
@@ -549,10 +615,21 @@ int choose_engines(sp_solver *s) {
     }
     const int dev = s->ctx->device;
     int rc;
-    if (s->sv_p64 >= 0 && (rc = StreamP64::prepare(dev))) return rc;
-    if (s->sv_d64 >= 0 && (rc = StreamD64::prepare(dev))) return rc;
-    if (s->mixed && s->sv_p32 >= 0 && (rc = StreamP32::prepare(dev))) return rc;
-    if (s->mixed && s->sv_d32 >= 0 && (rc = StreamD32::prepare(dev))) return rc;
+    // the SELL copies, where a pass uses them (a matrix with a row longer than a tile
+    // has none: its passes fall back to the tile engine)
+    const bool sell_p = s->sv_p64 == ENGINE_SELL || (s->mixed && s->sv_p32 == ENGINE_SELL);
+    const bool sell_d = s->sv_d64 == ENGINE_SELL || (s->mixed && s->sv_d32 == ENGINE_SELL);
+    if (sell_p && (rc = build_sell(s, s->AT, &s->sellAT))) return rc;
+    if (sell_d && (rc = build_sell(s, s->A, &s->sellA))) return rc;
+    for (int *v : {&s->sv_p64, &s->sv_p32})
+        if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;
+    for (int *v : {&s->sv_d64, &s->sv_d32})
+        if (*v == ENGINE_SELL && !s->sellA.ok) *v = -1;
+    auto stream = [](int v) { return v >= 0 && v < SV_COUNT; };
+    if (stream(s->sv_p64) && (rc = StreamP64::prepare(dev))) return rc;
+    if (stream(s->sv_d64) && (rc = StreamD64::prepare(dev))) return rc;
+    if (s->mixed && stream(s->sv_p32) && (rc = StreamP32::prepare(dev))) return rc;
+    if (s->mixed && stream(s->sv_d32) && (rc = StreamD32::prepare(dev))) return rc;
     return SP_OK;
 }
 
@@ -566,10 +643,12 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     const size_t sm = smem_P();
     if (role == ROLE_MID && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
         if (s->mixed) {
-            if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
+            if (s->sv_p32 == ENGINE_SELL) launch_sell(s->sellAT, st, mkP<true, 0>(p, i, role));
+            else if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
             else k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role));
         }
-        if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
+        if (s->sv_p64 == ENGINE_SELL) launch_sell(s->sellAT, st, mkP<false, 0>(p, i, role));
+        else if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
         else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
         return;
     }
@@ -602,10 +681,12 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
     if (role == ROLE_MID && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
         const size_t s1 = tile_smem_bytes<1, double>();
         if (s->mixed) {
-            if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
+            if (s->sv_d32 == ENGINE_SELL) launch_sell(s->sellA, st, mkD<true, 0>(p, i, role));
+            else if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
             else k_tiles_any<<<g, NT, s1, st>>>(mkD<true, 0>(p, i, role));
         }
-        if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
+        if (s->sv_d64 == ENGINE_SELL) launch_sell(s->sellA, st, mkD<false, 0>(p, i, role));
+        else if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
         else k_tiles_any<<<g, NT, s1, st>>>(mkD<false, 0>(p, i, role));
         return;
     }
@@ -719,6 +800,8 @@ void solver_release(sp_solver *s) {
     cudaStream_t fst = s->ctx->stream;
     free_csr(&s->A, fst);
     free_csr(&s->AT, fst);
+    free_sell(&s->sellA, fst);
+    free_sell(&s->sellAT, fst);
     void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
                     s->aty, s->xbar32, s->y32, s->pk, s->pky, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
                     s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "sell.cuh"
 
 namespace sp {
 constexpr int SolverLookahead = 2;  // epochs queued ahead of the state the host has read
@@ -17,8 +18,10 @@ struct sp_solver {
     sp_ctx *ctx = nullptr;
     sp_solver_params prm{};
     int mixed = 0;
-    // engine of each MID pass: -1 the tile engine, else a stream-engine variant (stream.cuh)
+    // engine of each MID pass: -1 the tile engine, ENGINE_SELL the SELL path (sell.cuh),
+    // else a stream-engine variant (stream.cuh)
     int sv_p64 = -1, sv_p32 = -1, sv_d64 = -1, sv_d32 = -1;
+    sp::SellMat sellA, sellAT;  // SELL copies of A' (dual pass) and A'ᵀ (primal pass), when used
     int64_t m = 0, n = 0, nnz = 0;
     double c0 = 0.0;
     int maximize = 0;

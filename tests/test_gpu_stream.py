@@ -100,6 +100,24 @@ def test_stream_engine_equals_tile_engine(variant, powerlaw_lp, gpu_backend):
                      solve_with("tiles", powerlaw_lp, params, gpu_backend))
 
 
+def test_sell_path_equals_tile_engine(powerlaw_lp, gpu_backend):
+    """SP_PASS_ENGINE=sell: every MID pass on its SELL copy (warp rows from CSR)."""
+    params = fixed_iterations(320)
+    assert_identical(solve_with("sell", powerlaw_lp, params, gpu_backend),
+                     solve_with("tiles", powerlaw_lp, params, gpu_backend))
+    params = fixed_iterations(320, sp().Precision.Mixed)
+    assert_identical(solve_with("sell", powerlaw_lp, params, gpu_backend),
+                     solve_with("tiles", powerlaw_lp, params, gpu_backend))
+
+
+def test_sell_path_with_warp_rows_and_empty_rows(gpu_backend):
+    # dense row of 1500 and dense column of 1800 entries (warp rows, no row beyond a tile),
+    # empty rows and columns, ragged slices
+    lp = ragged_lp(seed=11, m=2500, n=1800, empty_rows=700, empty_cols=300)
+    params = fixed_iterations(256)
+    assert_identical(solve_with("sell", lp, params, gpu_backend), solve_with("tiles", lp, params, gpu_backend))
+
+
 def test_stream_engine_mixed_form_equals_tile_engine(powerlaw_lp, gpu_backend):
     params = fixed_iterations(320, sp().Precision.Mixed)
     assert_identical(solve_with("stream", powerlaw_lp, params, gpu_backend),
