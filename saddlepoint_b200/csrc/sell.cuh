@@ -15,7 +15,8 @@
 
 namespace sp {
 
-constexpr int SELL_BATCH = 8;      // loads in flight per lane
+constexpr int SELL_BATCH = 8;                // loads in flight per lane
+constexpr int64_t SELL_MAX_SLOTS_PER_NNZ = 2;  // padding cap of a SELL copy (server footprints count it)
 constexpr uint8_t SELL_HEAVY = 0xFF;  // length mark of a row summed by a warp
 
 struct SellMat {

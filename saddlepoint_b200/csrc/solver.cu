@@ -530,8 +530,11 @@ using StreamP32 = StreamKernel<PrimalPass<true, 0>>;
 using StreamD64 = StreamKernel<DualPass<false, 0>>;
 using StreamD32 = StreamKernel<DualPass<true, 0>>;
 
+void free_sell(SellMat *S, cudaStream_t st);
+
 // The SELL copy of one matrix (sell.cuh), built on the device from its CSR arrays after
-// scaling. Left unbuilt (ok = false) for a matrix with a row longer than TILE_NNZ.
+// scaling. Left unbuilt (ok = false) for a matrix with a row longer than TILE_NNZ, or
+// whose slices would hold more than SELL_MAX_SLOTS_PER_NNZ slots per nonzero.
 int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     cudaStream_t st = s->ctx->stream;
     *S = SellMat{};
@@ -565,6 +568,12 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     S->slots = last[0] + last[1];
     S->nheavy = nh;
+    if (S->slots > SELL_MAX_SLOTS_PER_NNZ * std::max<int64_t>(M.nnz, 1024)) {
+        // rows too uneven for slices: more padding than the pass would save
+        for (void *p : {(void *)slots, (void *)flag, (void *)nsel, tmp}) dfree(p, st);
+        free_sell(S, st);
+        return SP_OK;
+    }
     if ((rc = dmalloc((void **)&S->ci, sizeof(int) * std::max<int64_t>(S->slots, 1))) ||
         (rc = dmalloc((void **)&S->v, sizeof(double) * std::max<int64_t>(S->slots, 1))))
         return rc;
