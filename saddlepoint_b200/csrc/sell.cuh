@@ -15,7 +15,6 @@
 
 namespace sp {
 
-constexpr int SELL_BATCH = 8;                // loads in flight per lane
 constexpr int64_t SELL_MAX_SLOTS_PER_NNZ = 2;  // padding cap of a SELL copy (server footprints count it)
 constexpr uint8_t SELL_HEAVY = 0xFF;  // length mark of a row summed by a warp
 
@@ -86,9 +85,9 @@ __global__ void k_sell_fill(const int *__restrict__ rp, const int *__restrict__ 
 }
 
 // A FUSED pass (NP = 0, one gathered vector) on the SELL copy: warps take the warp rows
-// first, then the slices, one item each.
-template <class Op>
-__global__ void __launch_bounds__(NT) k_sell(Op op, SellArgs S) {
+// first, then the slices, one item each. B loads in flight per lane; MINB CTAs per SM.
+template <class Op, int B, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell(Op op, SellArgs S) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
     using ST = typename Op::ST;
@@ -96,7 +95,6 @@ __global__ void __launch_bounds__(NT) k_sell(Op op, SellArgs S) {
     static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
     constexpr bool F32 = (Op::F32 & 1u) != 0;
     using AT = typename std::conditional<F32, float, double>::type;
-    constexpr int B = SELL_BATCH;
     if (!op.setup()) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t item = (int64_t)blockIdx.x * (NT / 32) + warp;

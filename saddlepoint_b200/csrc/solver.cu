@@ -592,11 +592,16 @@ void free_sell(SellMat *S, cudaStream_t st) {
     *S = SellMat{};
 }
 
+// SELL kernel shape, from a sweep on the 40M LP's dual pass: FP64 values with 8 loads in
+// flight per lane at the registers' natural occupancy (0.203 ms; 4 loads at 6 CTAs/SM
+// 0.201, 8 at 5 0.206), FP32 values with 4 loads at 6 CTAs/SM (0.190; 8 loads 0.200).
 template <class Op>
 void launch_sell(const SellMat &S, cudaStream_t st, const Op &op) {
     const SellArgs a{S.ci, S.v, S.v32, S.off, S.slen, S.len, S.heavy, S.nrows, S.nslices, S.nheavy};
     const int64_t items = S.nheavy + S.nslices;
-    k_sell<Op><<<(unsigned)((items + NT / 32 - 1) / (NT / 32)), NT, 0, st>>>(op, a);
+    const unsigned grid = (unsigned)((items + NT / 32 - 1) / (NT / 32));
+    if constexpr (sizeof(typename Op::VT) == 4) k_sell<Op, 4, 6><<<grid, NT, 0, st>>>(op, a);
+    else k_sell<Op, 8, 1><<<grid, NT, 0, st>>>(op, a);
 }
 
 // Which engine runs each MID pass (-1: the tile engine, ENGINE_SELL the SELL path, else a
