@@ -1,14 +1,30 @@
-// sell.cuh — the SELL-32 path of a FUSED pass over a matrix whose rows are short.
+// sell.cuh — the SELL path of a FUSED pass: short rows in slices of 32 sorted by length
+// inside windows (SELL-C-σ), warp rows as a stream of 32-entry chunks.
 //
-// The rows are cut into slices of 32 consecutive rows; a slice stores the entries of its
-// rows column-major (entry j of the slice's row `lane` at off + 32·j + lane), padded to its
-// longest row, so lane `lane` of a warp walks its own row with loads that are coalesced
-// across the warp, gathers the vector and sums in registers: no shared memory, no
-// barrier. Rows longer than SEQ_MAX are left out of the slices (length 0) and summed by
-// one warp each straight from the CSR arrays. Both sums are the tile engine's: a short
-// row from -0.0 in column order by one thread, a long row as lane-strided partials and
-// the fixed shuffle tree; so all engines give the same bits. The path is built only for
-// matrices without rows longer than TILE_NNZ (those need the CTA-wide tree).
+// Short rows (at most SEQ_MAX entries). The rows are cut into windows of SELL_WIN
+// consecutive rows; inside a window they are ordered by decreasing length (a stable order:
+// ties keep row order) and the ordered rows are cut into slices of 32. A slice stores the
+// entries of its rows column-major (entry j of the slice's row at position `lane` sits at
+// off + 32·j + lane), padded to its longest row, so lane `lane` of a warp walks its own row
+// with loads that are coalesced across the warp, gathers the vector and sums in registers.
+// Sorting keeps the padding — and the partly used sectors of the index/value loads — small
+// where row lengths vary. One CTA takes a window (k_sell_win): its warps sum the window's
+// slices, leave each sum in shared memory at the row's place in the window, and after one
+// barrier the CTA's threads run the epilogue in row order (row inputs and outputs coalesced).
+//
+// Warp rows (longer than SEQ_MAX, at most TILE_NNZ). Each is stored as whole chunks of 32
+// entries (the last one padded with column -1), the rows one after another in row order;
+// lane `lane` of a chunk holds entry lane + 32·chunk of its row. A warp takes a segment of
+// SELL_SEG consecutive warp rows (k_sell_rows) and streams their chunks BH at a time, the
+// next batch's index/value loads issued before this batch's sums, so neither row boundaries
+// nor the index loads stall the gathers; at each row's end the warp folds its lanes'
+// partials with the fixed shuffle tree and the lane holding that row's inputs runs its
+// epilogue. The two kernels write disjoint rows and run side by side on two streams.
+//
+// Both sums are the tile engine's: a short row from -0.0 in column order by one thread, a
+// warp row as lane-strided partials (lane k: entries k, k + 32, … in order) and the same
+// tree; so all engines give the same bits. The path is built only for matrices without rows
+// longer than TILE_NNZ (those need the CTA-wide tree).
 #pragma once
 
 #include "tiles.cuh"
@@ -16,67 +32,106 @@
 namespace sp {
 
 constexpr int64_t SELL_MAX_SLOTS_PER_NNZ = 2;  // padding cap of a SELL copy (server footprints count it)
-constexpr uint8_t SELL_HEAVY = 0xFF;  // length mark of a row summed by a warp
+constexpr uint8_t SELL_HEAVY = 0xFF;           // length mark of a warp row
+constexpr int SELL_WIN_SHIFT = 10;
+constexpr int SELL_WIN = 1 << SELL_WIN_SHIFT;        // rows per window: one CTA's work
+constexpr int SELL_SPW = SELL_WIN / 32 / (NT / 32);  // slices per warp in a window
+constexpr int SELL_SEG = 16;                         // warp rows per segment: one warp's work
+static_assert(SELL_WIN % NT == 0 && SELL_SPW >= 1, "a window is a whole number of slices per warp");
+static_assert(SELL_SEG < 32, "a segment's row bounds sit in one lane each");
 
 struct SellMat {
-    int64_t nrows = 0, nslices = 0, nheavy = 0, slots = 0;
-    int *ci = nullptr;       // [slots]
-    double *v = nullptr;     // [slots]
-    float *v32 = nullptr;    // [slots], mixed form
-    int64_t *off = nullptr;  // [nslices] first slot of each slice
-    int *slen = nullptr;     // [nslices] longest short row of each slice
-    uint8_t *len = nullptr;  // [nslices * 32] row lengths, SELL_HEAVY for warp rows
-    int *heavy = nullptr;    // [nheavy] the warp rows
+    int64_t nrows = 0, nwin = 0, nslices = 0, slots = 0;
+    int64_t nheavy = 0, nseg = 0, chunks = 0;
+    int *ci = nullptr;          // [slots] slices
+    double *v = nullptr;        // [slots]
+    float *v32 = nullptr;       // [slots], mixed form
+    int64_t *off = nullptr;     // [nslices] first slot of each slice
+    int *slen = nullptr;        // [nslices] longest row of each slice
+    uint8_t *len = nullptr;     // [nwin * SELL_WIN] row lengths in row order, SELL_HEAVY for warp rows
+    uint8_t *lsort = nullptr;   // [nwin * SELL_WIN] short row lengths in slice order (warp rows 0)
+    uint16_t *perm = nullptr;   // [nwin * SELL_WIN] row (within its window) at each slice position
+    int *heavy = nullptr;       // [nheavy] the warp rows, in row order
+    int64_t *choff = nullptr;   // [nheavy + 1] first chunk of each warp row
+    int *hci = nullptr;         // [chunks * 32] warp rows' columns, -1 past a row's end
+    double *hv = nullptr;       // [chunks * 32]
+    float *hv32 = nullptr;      // [chunks * 32], mixed form
     bool ok = false;
 };
 
-// Pointers of the SELL copy the kernel reads.
+// Pointers of the SELL copy the kernels read.
 struct SellArgs {
     const int *ci;
     const double *v;
     const float *v32;
     const int64_t *off;
     const int *slen;
-    const uint8_t *len;
+    const uint8_t *len, *lsort;
+    const uint16_t *perm;
     const int *heavy;
-    int64_t nrows, nslices, nheavy;
+    const int64_t *choff;
+    const int *hci;
+    const double *hv;
+    const float *hv32;
+    int64_t nrows, nwin, nheavy, nseg;
 };
 
-// One warp per slice: row lengths, warp rows flagged, the slice's longest short row and
-// its slot count (32 per entry of that row).
-__global__ void k_sell_meta(const int *__restrict__ rp, int64_t nrows, int64_t nslices, uint8_t *__restrict__ len,
-                            int *__restrict__ slen, int64_t *__restrict__ slots, int *__restrict__ heavy_flag) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; s < nslices;
-         s += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t r = s * 32 + lane;
+// Per row (the last window padded with empty rows): its length mark in row order, its
+// warp-row flag, and its sort key — the window, then 32 minus its short length — so that a
+// stable sort of the keys orders each window's rows by decreasing short length (warp rows
+// and padding count as 0) and keeps row order among equal lengths.
+__global__ void k_sell_keys(const int *__restrict__ rp, int64_t nrows, int64_t npad, uint8_t *__restrict__ len,
+                            int *__restrict__ heavy_flag, uint32_t *__restrict__ key, uint16_t *__restrict__ loc) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < npad; r += (int64_t)gridDim.x * blockDim.x) {
         const int l = r < nrows ? rp[r + 1] - rp[r] : 0;
         const bool heavy = l > SEQ_MAX;
-        const int ls = heavy ? 0 : l;
-        len[r] = heavy ? SELL_HEAVY : (uint8_t)ls;
+        len[r] = heavy ? SELL_HEAVY : (uint8_t)l;
         if (r < nrows) heavy_flag[r] = heavy ? 1 : 0;
-        const int mx = __reduce_max_sync(0xffffffffu, ls);
-        if (lane == 0) {
-            slen[s] = mx;
-            slots[s] = 32ll * mx;
+        key[r] = ((uint32_t)(r >> SELL_WIN_SHIFT) << 6) | (uint32_t)(32 - (heavy ? 0 : l));
+        loc[r] = (uint16_t)(r & (SELL_WIN - 1));
+    }
+}
+
+// Per slice position of the sorted keys: the short length there; per slice its width (its
+// first row is its longest) and slot count.
+__global__ void k_sell_slices(const uint32_t *__restrict__ skey, int64_t npad, uint8_t *__restrict__ lsort,
+                              int *__restrict__ slen, int64_t *__restrict__ slots) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < npad; k += (int64_t)gridDim.x * blockDim.x) {
+        const int l = 32 - (int)(skey[k] & 63u);
+        lsort[k] = (uint8_t)l;
+        if ((k & 31) == 0) {
+            slen[k >> 5] = l;
+            slots[k >> 5] = 32ll * l;
         }
     }
 }
 
-// One warp per slice: copies each short row's entries to its column-major slots.
+// Per warp row: its chunk count (entry h of nheavy + 1; the last is 0, for the scan's total).
+__global__ void k_sell_chunk_counts(const int *__restrict__ rp, const int *__restrict__ heavy, int64_t nheavy,
+                                    int64_t *__restrict__ cnt) {
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h <= nheavy; h += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = 0;
+        if (h < nheavy) {
+            const int r = heavy[h];
+            c = (rp[r + 1] - rp[r] + 31) / 32;
+        }
+        cnt[h] = c;
+    }
+}
+
+// One thread per slice position: copies its row's entries to their column-major slots.
 __global__ void k_sell_fill(const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
-                            int64_t nrows, int64_t nslices, const uint8_t *__restrict__ len,
+                            int64_t npad, const uint8_t *__restrict__ lsort, const uint16_t *__restrict__ perm,
                             const int64_t *__restrict__ off, int *__restrict__ sci, double *__restrict__ sv,
                             float *__restrict__ sv32) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; s < nslices;
-         s += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int64_t r = s * 32 + lane;
-        const int l = len[r];
-        if (r >= nrows || l == SELL_HEAVY) continue;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < npad; k += (int64_t)gridDim.x * blockDim.x) {
+        const int l = lsort[k];
+        if (l == 0) continue;
+        const int64_t r = ((k >> SELL_WIN_SHIFT) << SELL_WIN_SHIFT) + perm[k];
         const int a = rp[r];
+        const int64_t o = off[k >> 5] + (k & 31);
         for (int j = 0; j < l; ++j) {
-            const int64_t d = off[s] + 32ll * j + lane;
+            const int64_t d = o + 32ll * j;
             sci[d] = ci[a + j];
             sv[d] = v[a + j];
             if (sv32) sv32[d] = (float)v[a + j];
@@ -84,77 +139,183 @@ __global__ void k_sell_fill(const int *__restrict__ rp, const int *__restrict__ 
     }
 }
 
-// A FUSED pass (NP = 0, one gathered vector) on the SELL copy: warps take the warp rows
-// first, then the slices, one item each. B loads in flight per lane; MINB CTAs per SM.
-template <class Op, int B, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sell(Op op, SellArgs S) {
+// One warp per warp row: copies its entries to its chunks, padding the last with column -1.
+__global__ void k_sell_chunk_fill(const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
+                                  const int *__restrict__ heavy, int64_t nheavy, const int64_t *__restrict__ choff,
+                                  int *__restrict__ hci, double *__restrict__ hv, float *__restrict__ hv32) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t h = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; h < nheavy;
+         h += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int r = heavy[h];
+        const int a = rp[r], l = rp[r + 1] - a;
+        const int64_t base = choff[h] * 32;
+        const int n = (int)(choff[h + 1] - choff[h]) * 32;
+        for (int j = lane; j < n; j += 32) {
+            const bool in = j < l;
+            hci[base + j] = in ? ci[a + j] : -1;
+            const double x = in ? v[a + j] : 0.0;
+            hv[base + j] = x;
+            if (hv32) hv32[base + j] = (float)x;
+        }
+    }
+}
+
+// The warp rows of a FUSED pass (NP = 0, one gathered vector) on the SELL copy: one
+// segment per warp, up to 2·BH chunks in flight per lane; MINB CTAs per SM.
+template <class Op, int BH, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell_rows(Op op, SellArgs S) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
-    using ST = typename Op::ST;
     using Pre = typename Op::Pre;
     static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
     constexpr bool F32 = (Op::F32 & 1u) != 0;
     using AT = typename std::conditional<F32, float, double>::type;
     if (!op.setup()) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t item = (int64_t)blockIdx.x * (NT / 32) + warp;
     const GT *__restrict__ gv = op.gvec();
     double part[1] = {0.0};
-    if (item < S.nheavy) {
-        // a warp row straight from CSR: lane-strided partials in order, then the tree
-        const int r = S.heavy[item];
-        const int a = op.rp[r], b = op.rp[r + 1];
-        AT s = AT(-0.0);
-        for (int base = a + lane; base < b; base += 32 * B) {
-            int c[B];
-            VT v[B];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const int e = base + 32 * u;
-                if (e < b) {
-                    c[u] = ld_stream(op.ci + e);
-                    v[u] = ld_stream(op.vals + e);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < B; ++u)
-                if (base + 32 * u < b) s += AT(op.mul(v[u], __ldg(gv + c[u])));
-        }
-        const double sum[1] = {double(warp_sum_down(s))};
-        if (lane == 0) op.row(r, sum, part, op.pre(r));
-        return;
-    }
-    const int64_t sl = item - S.nheavy;
-    if (sl >= S.nslices) return;
-    const int64_t r = sl * 32 + lane;
-    const int lraw = S.len[r];
-    const bool live = r < S.nrows && lraw != SELL_HEAVY;
-    const int l = live ? lraw : 0;
+    const int64_t seg = (int64_t)blockIdx.x * (NT / 32) + warp;
+    if (seg >= S.nseg) return;
+    const int64_t h0 = seg * SELL_SEG;
+    const int nr = (int)(S.nheavy - h0 < SELL_SEG ? S.nheavy - h0 : SELL_SEG);
+    // lane k < nr: row k of the segment and its inputs; lanes 0..nr: the chunk bounds
+    int row = 0;
+    int64_t bound = 0;
     Pre pre{};
-    if (live) pre = op.pre((int)r);
-    const int L = S.slen[sl];
-    const int64_t off = S.off[sl] + lane;
+    if (lane <= nr) bound = S.choff[h0 + lane];
+    if (lane < nr) {
+        row = S.heavy[h0 + lane];
+        pre = op.pre(row);
+    }
+    const int64_t c0 = __shfl_sync(0xffffffffu, bound, 0), c1 = __shfl_sync(0xffffffffu, bound, nr);
+    const VT *__restrict__ hv;
+    if constexpr (sizeof(VT) == 4) hv = reinterpret_cast<const VT *>(S.hv32);
+    else hv = reinterpret_cast<const VT *>(S.hv);
+    int cur = 0;
+    AT s = AT(-0.0);
+    // row cur is complete: the tree, then its epilogue on the lane that holds it
+    auto finish = [&]() {
+        const AT tot = __shfl_sync(0xffffffffu, warp_sum_down(s), 0);
+        if (lane == cur) {
+            const double sum[1] = {double(tot)};
+            op.row(row, sum, part, pre);
+        }
+    };
+    const int *__restrict__ pc = S.hci + c0 * 32 + lane;
+    const VT *__restrict__ pv = hv + c0 * 32 + lane;
+    const int nch = (int)(c1 - c0);
+    int nxt = (int)(__shfl_sync(0xffffffffu, bound, 1) - c0);  // first chunk of row cur + 1
+    int c[BH];
+    VT v[BH];
+#pragma unroll
+    for (int u = 0; u < BH; ++u) {
+        c[u] = -1;
+        if (u < nch) {
+            c[u] = ld_stream(pc + 32 * u);
+            v[u] = ld_stream(pv + 32 * u);
+        }
+    }
+    for (int ch = 0; ch < nch; ch += BH) {
+        GT g[BH];
+#pragma unroll
+        for (int u = 0; u < BH; ++u)
+            if (c[u] >= 0) g[u] = __ldg(gv + c[u]);
+        pc += 32 * BH;
+        pv += 32 * BH;
+        int cn[BH];
+        VT vn[BH];
+#pragma unroll
+        for (int u = 0; u < BH; ++u) {
+            cn[u] = -1;
+            if (ch + BH + u < nch) {
+                cn[u] = ld_stream(pc + 32 * u);
+                vn[u] = ld_stream(pv + 32 * u);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < BH; ++u) {
+            if (ch + u >= nch) break;
+            if (ch + u == nxt) {  // a warp row spans at least two chunks
+                finish();
+                ++cur;
+                nxt = (int)(__shfl_sync(0xffffffffu, bound, cur + 1) - c0);
+                s = AT(-0.0);
+            }
+            if (c[u] >= 0) s += AT(op.mul(v[u], g[u]));
+        }
+#pragma unroll
+        for (int u = 0; u < BH; ++u) {
+            c[u] = cn[u];
+            v[u] = vn[u];
+        }
+    }
+    finish();
+}
+
+// The short rows of a FUSED pass (NP = 0, one gathered vector) on the SELL copy: one
+// window per CTA, BS slice entries in flight per lane; MINB CTAs per SM.
+template <class Op, int BS, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
+    using VT = typename Op::VT;
+    using GT = typename Op::GT;
+    using Pre = typename Op::Pre;
+    static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
+    constexpr bool F32 = (Op::F32 & 1u) != 0;
+    using AT = typename std::conditional<F32, float, double>::type;
+    constexpr int W = NT / 32;  // warps per CTA
+    __shared__ AT sums[SELL_WIN];
+    if (!op.setup()) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const GT *__restrict__ gv = op.gvec();
+    double part[1] = {0.0};
+    const int64_t win = blockIdx.x;
     const VT *__restrict__ sv;
     if constexpr (sizeof(VT) == 4) sv = reinterpret_cast<const VT *>(S.v32);
     else sv = reinterpret_cast<const VT *>(S.v);
-    AT s = AT(-0.0);
-    for (int j0 = 0; j0 < L; j0 += B) {
-        int c[B];
-        VT v[B];
+    // the window's slices, widest first, dealt to the warps back and forth so that each
+    // warp's widths add up to about the same
+#pragma unroll 1
+    for (int q = 0; q < SELL_SPW; ++q) {
+        const int ls = q * W + ((q & 1) ? W - 1 - warp : warp);
+        const int64_t sl = win * (SELL_WIN / 32) + ls;
+        const int64_t k = sl * 32 + lane;
+        const int l = S.lsort[k];
+        const int L = S.slen[sl];
+        const int64_t off = S.off[sl] + lane;
+        AT s = AT(-0.0);
+        for (int j0 = 0; j0 < L; j0 += BS) {
+            int c[BS];
+            VT v[BS];
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            if (j0 + u < l) {
-                c[u] = ld_stream(S.ci + off + 32ll * (j0 + u));
-                v[u] = ld_stream(sv + off + 32ll * (j0 + u));
+            for (int u = 0; u < BS; ++u) {
+                if (j0 + u < l) {
+                    c[u] = ld_stream(S.ci + off + 32ll * (j0 + u));
+                    v[u] = ld_stream(sv + off + 32ll * (j0 + u));
+                }
             }
-        }
 #pragma unroll
-        for (int u = 0; u < B; ++u)
-            if (j0 + u < l) s += AT(op.mul(v[u], __ldg(gv + c[u])));
+            for (int u = 0; u < BS; ++u)
+                if (j0 + u < l) s += AT(op.mul(v[u], __ldg(gv + c[u])));
+        }
+        sums[S.perm[k]] = s;
     }
-    if (live) {
-        const double sum[1] = {double(s)};
-        op.row((int)r, sum, part, pre);
+    // the epilogue in row order, row inputs loaded before the barrier
+    constexpr int RPT = SELL_WIN / NT;
+    const int64_t rbase = win * SELL_WIN + threadIdx.x;
+    Pre pre[RPT];
+    bool live[RPT];
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+        const int64_t r = rbase + u * NT;
+        live[u] = r < S.nrows && S.len[r] != SELL_HEAVY;
+        if (live[u]) pre[u] = op.pre((int)r);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+        if (!live[u]) continue;
+        const double sum[1] = {double(sums[threadIdx.x + u * NT])};
+        op.row((int)(rbase + u * NT), sum, part, pre[u]);
     }
 }
 

@@ -533,32 +533,58 @@ using StreamD32 = StreamKernel<DualPass<true, 0>>;
 void free_sell(SellMat *S, cudaStream_t st);
 
 // The SELL copy of one matrix (sell.cuh), built on the device from its CSR arrays after
-// scaling. Left unbuilt (ok = false) for a matrix with a row longer than TILE_NNZ, or
-// whose slices would hold more than SELL_MAX_SLOTS_PER_NNZ slots per nonzero.
+// scaling: the rows' sort keys and a stable radix sort of them (each window's rows by
+// decreasing length), the slice widths and slot offsets, the warp-row list and its chunk
+// offsets, then the two copies. Left unbuilt (ok = false) for a matrix with a row longer
+// than TILE_NNZ, or whose copy would hold more than SELL_MAX_SLOTS_PER_NNZ slots per nonzero.
 int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     cudaStream_t st = s->ctx->stream;
     *S = SellMat{};
     if (M.nlong > 0 || M.nrows == 0) return SP_OK;
-    const int64_t nrows = M.nrows, nslices = (nrows + 31) / 32;
+    const int64_t nrows = M.nrows, nwin = (nrows + SELL_WIN - 1) / SELL_WIN, npad = nwin * SELL_WIN;
+    const int64_t nslices = npad / 32;
     S->nrows = nrows;
+    S->nwin = nwin;
     S->nslices = nslices;
-    int64_t *slots = nullptr;
+    int64_t *slots = nullptr, *cnt = nullptr;
     int *flag = nullptr, *nsel = nullptr;
+    uint32_t *key = nullptr, *skey = nullptr;
+    uint16_t *loc = nullptr;
     void *tmp = nullptr;
+    auto release = [&] {
+        for (void *p : {(void *)slots, (void *)cnt, (void *)flag, (void *)nsel, (void *)key, (void *)skey,
+                        (void *)loc, tmp})
+            dfree(p, st);
+    };
+    auto fail = [&](int rc) {
+        release();
+        free_sell(S, st);
+        return rc;
+    };
     int rc;
-    if ((rc = dmalloc((void **)&S->len, nslices * 32)) || (rc = dmalloc((void **)&S->slen, sizeof(int) * nslices)) ||
+    if ((rc = dmalloc((void **)&S->len, npad)) || (rc = dmalloc((void **)&S->lsort, npad)) ||
+        (rc = dmalloc((void **)&S->perm, sizeof(uint16_t) * npad)) ||
+        (rc = dmalloc((void **)&S->slen, sizeof(int) * nslices)) ||
         (rc = dmalloc((void **)&S->off, sizeof(int64_t) * nslices)) ||
         (rc = dmalloc((void **)&slots, sizeof(int64_t) * nslices)) || (rc = dmalloc((void **)&flag, sizeof(int) * nrows)) ||
+        (rc = dmalloc((void **)&key, sizeof(uint32_t) * npad)) || (rc = dmalloc((void **)&skey, sizeof(uint32_t) * npad)) ||
+        (rc = dmalloc((void **)&loc, sizeof(uint16_t) * npad)) ||
         (rc = dmalloc((void **)&S->heavy, sizeof(int) * nrows)) || (rc = dmalloc((void **)&nsel, sizeof(int))))
-        return rc;
-    const int g = grid_of(s->ctx, nslices * 32);
-    k_sell_meta<<<g, NT, 0, st>>>(M.rp, nrows, nslices, S->len, S->slen, slots, flag);
-    size_t b1 = 0, b2 = 0;
+        return fail(rc);
+    const int g = grid_of(s->ctx, npad);
+    k_sell_keys<<<g, NT, 0, st>>>(M.rp, nrows, npad, S->len, flag, key, loc);
+    int end_bit = 6;  // the window number above the 6 bits of the length
+    while (end_bit < 32 && ((uint64_t)(nwin - 1) >> (end_bit - 6))) ++end_bit;
+    size_t b0 = 0, b1 = 0, b2 = 0;
     thrust::counting_iterator<int> rows(0);
-    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, b1, slots, S->off, (int)nslices, st));
+    SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, b0, key, skey, loc, S->perm, npad, 0, end_bit, st));
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, b1, slots, S->off, nslices, st));
     SP_CUDA_TRY(cub::DeviceSelect::Flagged(nullptr, b2, rows, flag, S->heavy, nsel, (int)nrows, st));
-    if ((rc = dmalloc(&tmp, std::max(b1, b2)))) return rc;
-    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, b1, slots, S->off, (int)nslices, st));
+    size_t btmp = std::max({b0, b1, b2});
+    if ((rc = dmalloc(&tmp, btmp))) return fail(rc);
+    SP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, b0, key, skey, loc, S->perm, npad, 0, end_bit, st));
+    k_sell_slices<<<g, NT, 0, st>>>(skey, npad, S->lsort, S->slen, slots);
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, b1, slots, S->off, nslices, st));
     SP_CUDA_TRY(cub::DeviceSelect::Flagged(tmp, b2, rows, flag, S->heavy, nsel, (int)nrows, st));
     int64_t last[2];
     int nh = 0;
@@ -568,48 +594,82 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     S->slots = last[0] + last[1];
     S->nheavy = nh;
-    if (S->slots > SELL_MAX_SLOTS_PER_NNZ * std::max<int64_t>(M.nnz, 1024)) {
-        // rows too uneven for slices: more padding than the pass would save
-        for (void *p : {(void *)slots, (void *)flag, (void *)nsel, tmp}) dfree(p, st);
-        free_sell(S, st);
-        return SP_OK;
+    S->nseg = (nh + SELL_SEG - 1) / SELL_SEG;
+    // the warp rows' chunk offsets
+    if ((rc = dmalloc((void **)&S->choff, sizeof(int64_t) * (nh + 1))) ||
+        (rc = dmalloc((void **)&cnt, sizeof(int64_t) * (nh + 1))))
+        return fail(rc);
+    k_sell_chunk_counts<<<grid_of(s->ctx, (int64_t)nh + 1), NT, 0, st>>>(M.rp, S->heavy, nh, cnt);
+    size_t b3 = 0;
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, b3, cnt, S->choff, (int64_t)nh + 1, st));
+    if (b3 > btmp) {
+        dfree(tmp, st);
+        tmp = nullptr;
+        if ((rc = dmalloc(&tmp, b3))) return fail(rc);
     }
+    SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, b3, cnt, S->choff, (int64_t)nh + 1, st));
+    SP_CUDA_TRY(cudaMemcpyAsync(&S->chunks, S->choff + nh, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    // rows too uneven for slices: more padding than the pass would save
+    if (S->slots + 32 * S->chunks > SELL_MAX_SLOTS_PER_NNZ * std::max<int64_t>(M.nnz, 1024)) return fail(SP_OK);
+    const int64_t hs = 32 * S->chunks;
     if ((rc = dmalloc((void **)&S->ci, sizeof(int) * std::max<int64_t>(S->slots, 1))) ||
-        (rc = dmalloc((void **)&S->v, sizeof(double) * std::max<int64_t>(S->slots, 1))))
-        return rc;
-    if (s->mixed && (rc = dmalloc((void **)&S->v32, sizeof(float) * std::max<int64_t>(S->slots, 1)))) return rc;
-    k_sell_fill<<<g, NT, 0, st>>>(M.rp, M.ci, M.v, nrows, nslices, S->len, S->off, S->ci, S->v, S->v32);
+        (rc = dmalloc((void **)&S->v, sizeof(double) * std::max<int64_t>(S->slots, 1))) ||
+        (s->mixed && (rc = dmalloc((void **)&S->v32, sizeof(float) * std::max<int64_t>(S->slots, 1)))) ||
+        (rc = dmalloc((void **)&S->hci, sizeof(int) * std::max<int64_t>(hs, 1))) ||
+        (rc = dmalloc((void **)&S->hv, sizeof(double) * std::max<int64_t>(hs, 1))) ||
+        (s->mixed && (rc = dmalloc((void **)&S->hv32, sizeof(float) * std::max<int64_t>(hs, 1)))))
+        return fail(rc);
+    k_sell_fill<<<g, NT, 0, st>>>(M.rp, M.ci, M.v, npad, S->lsort, S->perm, S->off, S->ci, S->v, S->v32);
+    if (nh > 0)
+        k_sell_chunk_fill<<<grid_of(s->ctx, 32 * (int64_t)nh), NT, 0, st>>>(M.rp, M.ci, M.v, S->heavy, nh, S->choff,
+                                                                             S->hci, S->hv, S->hv32);
     SP_CUDA_TRY(cudaGetLastError());
-    for (void *p : {(void *)slots, (void *)flag, (void *)nsel, tmp}) dfree(p, st);
+    release();
     S->ok = true;
     return SP_OK;
 }
 
 void free_sell(SellMat *S, cudaStream_t st) {
     for (void *p : {(void *)S->ci, (void *)S->v, (void *)S->v32, (void *)S->off, (void *)S->slen, (void *)S->len,
-                    (void *)S->heavy})
+                    (void *)S->lsort, (void *)S->perm, (void *)S->heavy, (void *)S->choff, (void *)S->hci,
+                    (void *)S->hv, (void *)S->hv32})
         dfree(p, st);
     *S = SellMat{};
 }
 
-// SELL kernel shape, from a sweep on the 40M LP's dual pass: FP64 values with 8 loads in
-// flight per lane at the registers' natural occupancy (0.203 ms; 4 loads at 6 CTAs/SM
-// 0.201, 8 at 5 0.206), FP32 values with 4 loads at 6 CTAs/SM (0.190; 8 loads 0.200).
+// A SELL pass: the warp rows on the solver's second stream, beside the windows on the
+// pass's stream (they write disjoint rows), joined before the next pass. Kernel shapes
+// from a sweep on the 40M LP (ms per pass, SELL path for both passes): warp rows with 2
+// chunks per batch at 4 CTAs/SM in FP64 (primal pass 0.276; 4 chunks at 3 CTAs/SM 0.290,
+// 4 or 8 at the registers' natural occupancy 0.288–0.293), 4 at 4 CTAs/SM in FP32 (0.255;
+// 2 chunks 0.264); windows with 8 slice entries in flight at 4 CTAs/SM in both (dual pass
+// 0.193 FP64, 0.191 FP32; 4 entries 0.198, 8 at natural occupancy 0.207, 16 0.233).
 template <class Op>
-void launch_sell(const SellMat &S, cudaStream_t st, const Op &op) {
-    const SellArgs a{S.ci, S.v, S.v32, S.off, S.slen, S.len, S.heavy, S.nrows, S.nslices, S.nheavy};
-    const int64_t items = S.nheavy + S.nslices;
-    const unsigned grid = (unsigned)((items + NT / 32 - 1) / (NT / 32));
-    if constexpr (sizeof(typename Op::VT) == 4) k_sell<Op, 4, 6><<<grid, NT, 0, st>>>(op, a);
-    else k_sell<Op, 8, 1><<<grid, NT, 0, st>>>(op, a);
+void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) {
+    const SellArgs a{S.ci,    S.v,   S.v32, S.off,  S.slen,  S.len,  S.lsort,  S.perm, S.heavy,
+                     S.choff, S.hci, S.hv,  S.hv32, S.nrows, S.nwin, S.nheavy, S.nseg};
+    const bool rows = S.nseg > 0;
+    if (rows) {
+        cudaEventRecord(s->fork, st);
+        cudaStreamWaitEvent(s->aux, s->fork, 0);
+        const unsigned gr = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32));
+        if constexpr (sizeof(typename Op::VT) == 4) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        else k_sell_rows<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
+    }
+    k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    if (rows) {
+        cudaEventRecord(s->join, s->aux);
+        cudaStreamWaitEvent(st, s->join, 0);
+    }
 }
 
 // Which engine runs each MID pass (-1: the tile engine, ENGINE_SELL the SELL path, else a
 // stream-engine variant). The defaults are the fastest measured on the 40M power-law LP (ms
 // per launch): the primal pass on the stream engine with 4 register-gatherer warps, 4 slots
-// in FP64 (0.255; tile engine 0.297, SELL 0.442 — its short rows are too uneven for slices)
-// and 4 in FP32 (0.247); the dual pass on its SELL copy in both precisions
-// (0.199 FP64, 0.208 FP32; tile engine 0.238 and 0.249, stream engine 0.300 and 0.227).
+// in FP64 (0.255; tile engine 0.297, SELL 0.276 — 69 % of its nonzeros sit in warp rows)
+// and 4 in FP32 (0.247; SELL 0.255); the dual pass on its SELL copy in both precisions
+// (0.193 FP64, 0.191 FP32; tile engine 0.238 and 0.249, stream engine 0.300 and 0.227).
 // SP_PASS_ENGINE=tiles|stream|sell overrides all four; SP_STREAM_GATHER names the
 // stream variant.
 int choose_engines(sp_solver *s) {
@@ -639,6 +699,11 @@ int choose_engines(sp_solver *s) {
         if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;
     for (int *v : {&s->sv_d64, &s->sv_d32})
         if (*v == ENGINE_SELL && !s->sellA.ok) *v = -1;
+    if ((s->sellA.ok || s->sellAT.ok) && !s->aux) {
+        SP_CUDA_TRY(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+        SP_CUDA_TRY(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+        SP_CUDA_TRY(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
+    }
     auto stream = [](int v) { return v >= 0 && v < SV_COUNT; };
     if (stream(s->sv_p64) && (rc = StreamP64::prepare(dev))) return rc;
     if (stream(s->sv_d64) && (rc = StreamD64::prepare(dev))) return rc;
@@ -657,11 +722,11 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     const size_t sm = smem_P();
     if (role == ROLE_MID && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
         if (s->mixed) {
-            if (s->sv_p32 == ENGINE_SELL) launch_sell(s->sellAT, st, mkP<true, 0>(p, i, role));
+            if (s->sv_p32 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<true, 0>(p, i, role));
             else if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
             else k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role));
         }
-        if (s->sv_p64 == ENGINE_SELL) launch_sell(s->sellAT, st, mkP<false, 0>(p, i, role));
+        if (s->sv_p64 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<false, 0>(p, i, role));
         else if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
         else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
         return;
@@ -695,11 +760,11 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
     if (role == ROLE_MID && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
         const size_t s1 = tile_smem_bytes<1, double>();
         if (s->mixed) {
-            if (s->sv_d32 == ENGINE_SELL) launch_sell(s->sellA, st, mkD<true, 0>(p, i, role));
+            if (s->sv_d32 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<true, 0>(p, i, role));
             else if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
             else k_tiles_any<<<g, NT, s1, st>>>(mkD<true, 0>(p, i, role));
         }
-        if (s->sv_d64 == ENGINE_SELL) launch_sell(s->sellA, st, mkD<false, 0>(p, i, role));
+        if (s->sv_d64 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<false, 0>(p, i, role));
         else if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
         else k_tiles_any<<<g, NT, s1, st>>>(mkD<false, 0>(p, i, role));
         return;
@@ -811,6 +876,12 @@ void solver_release(sp_solver *s) {
     cudaStreamSynchronize(s->ctx->stream);
     for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
     for (cudaEvent_t e : s->event_pool) cudaEventDestroy(e);
+    if (s->aux) {
+        cudaStreamSynchronize(s->aux);
+        cudaStreamDestroy(s->aux);
+        cudaEventDestroy(s->fork);
+        cudaEventDestroy(s->join);
+    }
     cudaStream_t fst = s->ctx->stream;
     free_csr(&s->A, fst);
     free_csr(&s->AT, fst);

@@ -22,6 +22,8 @@ struct sp_solver {
     // else a stream-engine variant (stream.cuh)
     int sv_p64 = -1, sv_p32 = -1, sv_d64 = -1, sv_d32 = -1;
     sp::SellMat sellA, sellAT;  // SELL copies of A' (dual pass) and A'ᵀ (primal pass), when used
+    cudaStream_t aux = nullptr;  // second stream of a SELL pass: its warp rows beside its windows
+    cudaEvent_t fork = nullptr, join = nullptr;
     int64_t m = 0, n = 0, nnz = 0;
     double c0 = 0.0;
     int maximize = 0;
