@@ -260,7 +260,9 @@ extern "C" int sp_ctx_create(int ordinal, sp_ctx **out) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_partials, sizeof(double) * RED_BLOCKS * RED_SLOTS * 4) != cudaSuccess ||
         cudaMalloc(&ctx->d_result, sizeof(double) * RED_SLOTS * 4) != cudaSuccess ||
-        cudaMallocHost(&ctx->h_result, sizeof(double) * RED_SLOTS * 4) != cudaSuccess) {
+        cudaMallocHost(&ctx->h_result, sizeof(double) * RED_SLOTS * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->d_tiles, sizeof(int) * 2) != cudaSuccess ||
+        cudaMemsetAsync(ctx->d_tiles, 0, sizeof(int) * 2, ctx->stream) != cudaSuccess) {
         cudaGetLastError();
         sp_ctx_destroy(ctx);
         return SP_ERR_UNAVAILABLE;
@@ -276,6 +278,7 @@ extern "C" void sp_ctx_destroy(sp_ctx *ctx) {
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_result);
     cudaFreeHost(ctx->h_result);
+    cudaFree(ctx->d_tiles);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (t_ctx_is(ctx)) set_current_ctx(nullptr);
     delete ctx;

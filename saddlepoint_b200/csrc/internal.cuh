@@ -16,6 +16,7 @@ struct sp_ctx {
     double *d_partials = nullptr;  // stage-one partials of the trait-method reductions
     double *d_result = nullptr;    // their final values
     double *h_result = nullptr;    // pinned copy read by the host
+    int *d_tiles = nullptr;        // work counters of the tile launches on `stream` (tiles.cuh: run_tiles)
 };
 
 struct sp_vec {

@@ -724,31 +724,31 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
         if (s->mixed) {
             if (s->sv_p32 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<true, 0>(p, i, role));
             else if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
-            else k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role));
+            else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 0>(p, i, role));
         }
         if (s->sv_p64 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<false, 0>(p, i, role));
         else if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
-        else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
+        else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 0>(p, i, role));
         return;
     }
     if (s->mixed) {
         if (role == ROLE_MID)
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
         else if (role == ROLE_FIRST) {
             // FUSED and K0 as launches of their own (one of them returns at once), so
             // the FUSED one keeps its own register and shared-memory footprint
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 1>(p, i, role), mkP<false, 1>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 0>(p, i, role), mkP<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 1>(p, i, role), mkP<false, 1>(p, i, role));
         }
         else
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<true, 2>(p, i, role), mkP<false, 2>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 2>(p, i, role), mkP<false, 2>(p, i, role));
     } else {
-        if (role == ROLE_MID) k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
+        if (role == ROLE_MID) launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 0>(p, i, role));
         else if (role == ROLE_FIRST) {
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 0>(p, i, role));
-            k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 1>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 1>(p, i, role));
         }
-        else k_tiles_any<<<g, NT, sm, st>>>(mkP<false, 2>(p, i, role));
+        else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 2>(p, i, role));
     }
 }
 
@@ -762,30 +762,30 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
         if (s->mixed) {
             if (s->sv_d32 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<true, 0>(p, i, role));
             else if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
-            else k_tiles_any<<<g, NT, s1, st>>>(mkD<true, 0>(p, i, role));
+            else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, s1, st, mkD<true, 0>(p, i, role));
         }
         if (s->sv_d64 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<false, 0>(p, i, role));
         else if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
-        else k_tiles_any<<<g, NT, s1, st>>>(mkD<false, 0>(p, i, role));
+        else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, s1, st, mkD<false, 0>(p, i, role));
         return;
     }
     if (s->mixed) {
         if (role == ROLE_MID)
-            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<1, double>(), st, mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
         else if (role == ROLE_FIRST) {
-            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
-            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<true, 1>(p, i, role), mkD<false, 1>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<1, double>(), st, mkD<true, 0>(p, i, role), mkD<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<2, double>(), st, mkD<true, 1>(p, i, role), mkD<false, 1>(p, i, role));
         }
         else
-            k_tiles_any<<<g, NT, sm, st>>>(mkD<true, 2>(p, i, role), mkD<false, 2>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkD<true, 2>(p, i, role), mkD<false, 2>(p, i, role));
     } else {
         if (role == ROLE_MID)
-            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<1, double>(), st, mkD<false, 0>(p, i, role));
         else if (role == ROLE_FIRST) {
-            k_tiles_any<<<g, NT, tile_smem_bytes<1, double>(), st>>>(mkD<false, 0>(p, i, role));
-            k_tiles_any<<<g, NT, tile_smem_bytes<2, double>(), st>>>(mkD<false, 1>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<1, double>(), st, mkD<false, 0>(p, i, role));
+            launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<2, double>(), st, mkD<false, 1>(p, i, role));
         }
-        else k_tiles_any<<<g, NT, sm, st>>>(mkD<false, 2>(p, i, role));
+        else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkD<false, 2>(p, i, role));
     }
 }
 
@@ -800,7 +800,7 @@ void launch_T(sp_solver *s, int i, cudaStream_t st) {
     o.sched = p.t_sched;
     o.s = p;
     o.i = i;
-    k_tiles_any<<<s->AT.ntiles, NT, smem_T(), st>>>(o);
+    launch_tiles(s->ctx->sms, s->ctx->d_tiles, s->AT.ntiles, smem_T(), st, o);
 }
 
 // One epoch of E iterations (the last is the check) on stream `st`. With timing

@@ -21,6 +21,9 @@
 // Everything is deterministic: the same inputs give the same bits on every run.
 #pragma once
 
+#include <map>
+#include <mutex>
+
 #include <algorithm>
 #include <cstdint>
 #include <thread>
@@ -162,20 +165,42 @@ constexpr size_t tile_smem_bytes() {
     return (size_t)G * TILE_NNZ * sizeof(ST) + (TILE_ROWS + 1) * sizeof(int);
 }
 
-// Sum of products [a, b) of slot q in accumulation type AT, in order, from -0.0.
-template <class AT, class ST>
-__device__ __forceinline__ AT seq_sum(const ST *__restrict__ p, int a, int b) {
-    AT s = AT(-0.0);
-    for (int e = a; e < b; ++e) s += AT(p[e]);
-    return s;
+// All G slots' sums of products [a, b) in one walk (slot q in float when bit q of F32 is
+// set): each slot is still summed in order from -0.0, but the G chains of adds overlap.
+template <int G, unsigned F32, class ST>
+__device__ __forceinline__ void seq_sums(const ST *__restrict__ p, int a, int b, double (&s)[G]) {
+    float sf[G];
+    double sd[G];
+#pragma unroll
+    for (int q = 0; q < G; ++q) { sf[q] = -0.0f; sd[q] = -0.0; }
+    for (int e = a; e < b; ++e) {
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            if ((F32 >> q) & 1u) sf[q] += float(p[q * TILE_NNZ + e]);
+            else sd[q] += double(p[q * TILE_NNZ + e]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < G; ++q) s[q] = ((F32 >> q) & 1u) ? double(sf[q]) : sd[q];
 }
 
-// Lane-strided partial sums then a shuffle tree; lane 0 gets the row sum.
-template <class AT, class ST>
-__device__ __forceinline__ AT warp_row_sum(const ST *__restrict__ p, int a, int b, int lane) {
-    AT s = AT(-0.0);
-    for (int e = a + lane; e < b; e += 32) s += AT(p[e]);
-    return warp_sum_down(s);
+// The same for a warp row: lane-strided partials of all G slots in one walk, then each
+// slot's shuffle tree; lane 0 gets the sums.
+template <int G, unsigned F32, class ST>
+__device__ __forceinline__ void warp_row_sums(const ST *__restrict__ p, int a, int b, int lane, double (&s)[G]) {
+    float sf[G];
+    double sd[G];
+#pragma unroll
+    for (int q = 0; q < G; ++q) { sf[q] = -0.0f; sd[q] = -0.0; }
+    for (int e = a + lane; e < b; e += 32) {
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            if ((F32 >> q) & 1u) sf[q] += float(p[q * TILE_NNZ + e]);
+            else sd[q] += double(p[q * TILE_NNZ + e]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < G; ++q) s[q] = ((F32 >> q) & 1u) ? double(warp_sum_down(sf[q])) : warp_sum_down(sd[q]);
 }
 
 // Streaming loads of the matrix: each element is read once per pass, so they are
@@ -299,10 +324,7 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
             const int a = srp[i], b = srp[i + 1];
             if (sched ? !(e & SCHED_WARP) : b - a <= SEQ_MAX) {
                 double s[G];
-#pragma unroll
-                for (int q = 0; q < G; ++q)
-                    s[q] = ((F32 >> q) & 1u) ? double(seq_sum<float>(prod + q * TILE_NNZ, a, b))
-                                             : seq_sum<double>(prod + q * TILE_NNZ, a, b);
+                seq_sums<G, F32>(prod, a, b, s);
                 if (u == tid) op.row(r0 + i, s, part, pre);
                 else op.row(r0 + i, s, part, op.pre(r0 + i));
             }
@@ -312,10 +334,7 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
         auto warp_row = [&](int i) {
             const int a = srp[i], b = srp[i + 1];
             double s[G];
-#pragma unroll
-            for (int q = 0; q < G; ++q)
-                s[q] = ((F32 >> q) & 1u) ? double(warp_row_sum<float>(prod + q * TILE_NNZ, a, b, lane))
-                                         : warp_row_sum<double>(prod + q * TILE_NNZ, a, b, lane);
+            warp_row_sums<G, F32>(prod, a, b, lane, s);
             if (lane == 0) op.row(r0 + i, s, part, op.pre(r0 + i));
         };
         if (sched) {
@@ -342,13 +361,65 @@ __device__ __forceinline__ void tile_body(Op &op, unsigned char *smem, int tile)
     }
 }
 
-// One CTA per tile. Op::setup() reads the device state and returns false when
-// the pass has nothing to do (solve finished, or a role this epoch skips).
+// The tiles of one launch. CTA b takes tile b, then whichever tile is next: ctr[0] counts
+// the tiles handed out beyond the first gridDim.x. Tiles are independent and each writes
+// its own rows and partial sums, so which CTA takes a tile changes no bit.
+template <class Op>
+__device__ __forceinline__ void run_tiles(Op &op, unsigned char *smem, int ntiles, int *ctr) {
+    __shared__ int next;
+    for (int t = blockIdx.x; t < ntiles;) {
+        tile_body(op, smem, t);
+        __syncthreads();  // the tile is done with shared memory
+        if (threadIdx.x == 0) next = (int)gridDim.x + atomicAdd(ctr, 1);
+        __syncthreads();
+        t = next;
+    }
+}
+
+// Every CTA of a tile launch ends here, whether or not its pass ran: the last one out
+// puts both counters back to zero for the next launch on the stream.
+__device__ __forceinline__ void tiles_exit(int *ctr) {
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's last hand-out before its exit count
+        if (atomicAdd(ctr + 1, 1) == (int)gridDim.x - 1) {
+            atomicExch(ctr, 0);
+            atomicExch(ctr + 1, 0);
+        }
+    }
+}
+
+// One CTA per tile. Op::setup() reads the device state and returns false when the pass
+// has nothing to do (solve finished, or a role this epoch skips).
 template <class Op>
 __global__ void __launch_bounds__(NT) k_tiles(Op op) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (!op.setup()) return;
     tile_body(op, smem, blockIdx.x);
 }
+
+// Grid of a persistent tile launch: one CTA per tile, up to as many as the device holds
+// at once (then each CTA takes tiles from the launch's counter until none are left). The
+// occupancy query is cached per kernel and shared-memory size.
+inline unsigned tile_grid(const void *kernel, int sms, int ntiles, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, size_t>, int> per_sm;
+    int bps = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = per_sm.find({kernel, smem});
+        if (it != per_sm.end()) {
+            bps = it->second;
+        } else {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, NT, smem) != cudaSuccess) {
+                cudaGetLastError();
+                bps = 0;
+            }
+            per_sm[{kernel, smem}] = bps;
+        }
+    }
+    const int64_t cap = (int64_t)bps * sms;
+    return (unsigned)(cap > 0 && cap < ntiles ? cap : ntiles);
+}
+
 
 }  // namespace sp
