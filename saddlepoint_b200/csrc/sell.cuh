@@ -14,12 +14,15 @@
 //
 // Warp rows (longer than SEQ_MAX, at most TILE_NNZ). Each is stored as whole chunks of 32
 // entries (the last one padded with column -1), the rows one after another in row order;
-// lane `lane` of a chunk holds entry lane + 32·chunk of its row. A warp takes a segment of
-// SELL_SEG consecutive warp rows (k_sell_rows) and streams their chunks BH at a time, the
-// next batch's index/value loads issued before this batch's sums, so neither row boundaries
-// nor the index loads stall the gathers; at each row's end the warp folds its lanes'
-// partials with the fixed shuffle tree and the lane holding that row's inputs runs its
-// epilogue. The two kernels write disjoint rows and run side by side on two streams.
+// lane `lane` of a chunk holds entry lane + 32·chunk of its row. The chunks are cut into
+// blocks of SELL_SEG_CHUNKS; a warp takes the rows that start in one block — a segment, at
+// most SELL_SEG_CHUNKS / 2 rows since each has at least two chunks — (k_sell_rows) and
+// streams their chunks BH at a time, the next batch's index/value loads issued before this
+// batch's sums, so neither row boundaries nor the index loads stall the gathers; at each
+// row's end the warp folds its lanes' partials with the fixed shuffle tree and the lane
+// holding that row's inputs runs its epilogue. On a large pass the two kernels write
+// disjoint rows and run side by side on two streams; a small pass runs both in one launch
+// (k_sell_both), whose fixed cost is one kernel.
 //
 // Both sums are the tile engine's: a short row from -0.0 in column order by one thread, a
 // warp row as lane-strided partials (lane k: entries k, k + 32, … in order) and the same
@@ -36,13 +39,14 @@ constexpr uint8_t SELL_HEAVY = 0xFF;           // length mark of a warp row
 constexpr int SELL_WIN_SHIFT = 10;
 constexpr int SELL_WIN = 1 << SELL_WIN_SHIFT;        // rows per window: one CTA's work
 constexpr int SELL_SPW = SELL_WIN / 32 / (NT / 32);  // slices per warp in a window
-constexpr int SELL_SEG = 16;                         // warp rows per segment: one warp's work
+constexpr int SELL_SEG_CHUNKS = 32;                  // chunks per block: a warp takes the rows starting in one
 static_assert(SELL_WIN % NT == 0 && SELL_SPW >= 1, "a window is a whole number of slices per warp");
-static_assert(SELL_SEG < 32, "a segment's row bounds sit in one lane each");
+static_assert(SELL_SEG_CHUNKS / 2 < 32, "a segment's row bounds sit in one lane each");
 
 struct SellMat {
     int64_t nrows = 0, nwin = 0, nslices = 0, slots = 0;
     int64_t nheavy = 0, nseg = 0, chunks = 0;
+    bool split = false;         // rows and windows as two launches on two streams (a large pass)
     int *ci = nullptr;          // [slots] slices
     double *v = nullptr;        // [slots]
     float *v32 = nullptr;       // [slots], mixed form
@@ -53,6 +57,7 @@ struct SellMat {
     uint16_t *perm = nullptr;   // [nwin * SELL_WIN] row (within its window) at each slice position
     int *heavy = nullptr;       // [nheavy] the warp rows, in row order
     int64_t *choff = nullptr;   // [nheavy + 1] first chunk of each warp row
+    int *segrow = nullptr;      // [nseg + 1] first warp row of each segment
     int *hci = nullptr;         // [chunks * 32] warp rows' columns, -1 past a row's end
     double *hv = nullptr;       // [chunks * 32]
     float *hv32 = nullptr;      // [chunks * 32], mixed form
@@ -70,6 +75,7 @@ struct SellArgs {
     const uint16_t *perm;
     const int *heavy;
     const int64_t *choff;
+    const int *segrow;
     const int *hci;
     const double *hv;
     const float *hv32;
@@ -119,6 +125,22 @@ __global__ void k_sell_chunk_counts(const int *__restrict__ rp, const int *__res
     }
 }
 
+// Per segment k (and the end, k = nseg): its first warp row, the first whose first chunk is
+// at or past k·SELL_SEG_CHUNKS (a binary search over the chunk offsets).
+__global__ void k_sell_segments(const int64_t *__restrict__ choff, int64_t nheavy, int64_t nseg,
+                                int *__restrict__ segrow) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nseg; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = k * SELL_SEG_CHUNKS;
+        int64_t lo = 0, hi = nheavy;  // choff[nheavy] is the total: every block start is at most it
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) / 2;
+            if (choff[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        segrow[k] = (int)(k == nseg ? nheavy : lo);
+    }
+}
+
 // One thread per slice position: copies its row's entries to their column-major slots.
 __global__ void k_sell_fill(const int *__restrict__ rp, const int *__restrict__ ci, const double *__restrict__ v,
                             int64_t npad, const uint8_t *__restrict__ lsort, const uint16_t *__restrict__ perm,
@@ -160,24 +182,22 @@ __global__ void k_sell_chunk_fill(const int *__restrict__ rp, const int *__restr
     }
 }
 
-// The warp rows of a FUSED pass (NP = 0, one gathered vector) on the SELL copy: one
-// segment per warp, up to 2·BH chunks in flight per lane; MINB CTAs per SM.
-template <class Op, int BH, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sell_rows(Op op, SellArgs S) {
+// The warp rows of segment `seg` of a FUSED pass (NP = 0, one gathered vector) on the SELL
+// copy, by one warp: up to 2·BH chunks in flight per lane.
+template <class Op, int BH>
+__device__ __forceinline__ void sell_rows_body(Op &op, const SellArgs &S, int64_t seg) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
     using Pre = typename Op::Pre;
     static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
     constexpr bool F32 = (Op::F32 & 1u) != 0;
     using AT = typename std::conditional<F32, float, double>::type;
-    if (!op.setup()) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     const GT *__restrict__ gv = op.gvec();
     double part[1] = {0.0};
-    const int64_t seg = (int64_t)blockIdx.x * (NT / 32) + warp;
-    if (seg >= S.nseg) return;
-    const int64_t h0 = seg * SELL_SEG;
-    const int nr = (int)(S.nheavy - h0 < SELL_SEG ? S.nheavy - h0 : SELL_SEG);
+    const int64_t h0 = S.segrow[seg];
+    const int nr = S.segrow[seg + 1] - (int)h0;
+    if (nr == 0) return;  // a block inside one long row
     // lane k < nr: row k of the segment and its inputs; lanes 0..nr: the chunk bounds
     int row = 0;
     int64_t bound = 0;
@@ -252,10 +272,18 @@ __global__ void __launch_bounds__(NT, MINB) k_sell_rows(Op op, SellArgs S) {
     finish();
 }
 
-// The short rows of a FUSED pass (NP = 0, one gathered vector) on the SELL copy: one
-// window per CTA, BS slice entries in flight per lane; MINB CTAs per SM.
-template <class Op, int BS, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
+// The warp rows of a FUSED pass on the SELL copy: one segment per warp; MINB CTAs per SM.
+template <class Op, int BH, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell_rows(Op op, SellArgs S) {
+    if (!op.setup()) return;
+    const int64_t seg = (int64_t)blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+    if (seg < S.nseg) sell_rows_body<Op, BH>(op, S, seg);
+}
+
+// The short rows of window `win` of a FUSED pass (NP = 0, one gathered vector) on the SELL
+// copy, by one CTA: BS slice entries in flight per lane.
+template <class Op, int BS>
+__device__ __forceinline__ void sell_win_body(Op &op, const SellArgs &S, int64_t win) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
     using Pre = typename Op::Pre;
@@ -264,11 +292,9 @@ __global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
     using AT = typename std::conditional<F32, float, double>::type;
     constexpr int W = NT / 32;  // warps per CTA
     __shared__ AT sums[SELL_WIN];
-    if (!op.setup()) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const GT *__restrict__ gv = op.gvec();
     double part[1] = {0.0};
-    const int64_t win = blockIdx.x;
     const VT *__restrict__ sv;
     if constexpr (sizeof(VT) == 4) sv = reinterpret_cast<const VT *>(S.v32);
     else sv = reinterpret_cast<const VT *>(S.v);
@@ -316,6 +342,27 @@ __global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
         if (!live[u]) continue;
         const double sum[1] = {double(sums[threadIdx.x + u * NT])};
         op.row((int)(rbase + u * NT), sum, part, pre[u]);
+    }
+}
+
+// The short rows of a FUSED pass on the SELL copy: one window per CTA; MINB CTAs per SM.
+template <class Op, int BS, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
+    if (!op.setup()) return;
+    sell_win_body<Op, BS>(op, S, blockIdx.x);
+}
+
+// Both parts of a small FUSED pass in one launch: the first ceil(nseg / 8) CTAs take the
+// segments, the rest the windows.
+template <class Op, int BH, int BS, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_sell_both(Op op, SellArgs S) {
+    if (!op.setup()) return;
+    const int64_t hb = (S.nseg + NT / 32 - 1) / (NT / 32);
+    if ((int64_t)blockIdx.x < hb) {
+        const int64_t seg = (int64_t)blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+        if (seg < S.nseg) sell_rows_body<Op, BH>(op, S, seg);
+    } else {
+        sell_win_body<Op, BS>(op, S, blockIdx.x - hb);
     }
 }
 

@@ -532,6 +532,10 @@ using StreamD32 = StreamKernel<DualPass<true, 0>>;
 
 void free_sell(SellMat *S, cudaStream_t st);
 
+// Passes over at least this many nonzeros run their SELL parts on two streams; smaller
+// ones in one launch (on small LPs an iteration's time is mostly launch latency).
+constexpr int64_t SELL_SPLIT_NNZ = 4 << 20;
+
 // The SELL copy of one matrix (sell.cuh), built on the device from its CSR arrays after
 // scaling: the rows' sort keys and a stable radix sort of them (each window's rows by
 // decreasing length), the slice widths and slot offsets, the warp-row list and its chunk
@@ -594,7 +598,6 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     S->slots = last[0] + last[1];
     S->nheavy = nh;
-    S->nseg = (nh + SELL_SEG - 1) / SELL_SEG;
     // the warp rows' chunk offsets
     if ((rc = dmalloc((void **)&S->choff, sizeof(int64_t) * (nh + 1))) ||
         (rc = dmalloc((void **)&cnt, sizeof(int64_t) * (nh + 1))))
@@ -610,6 +613,10 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
     SP_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, b3, cnt, S->choff, (int64_t)nh + 1, st));
     SP_CUDA_TRY(cudaMemcpyAsync(&S->chunks, S->choff + nh, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     SP_CUDA_TRY(cudaStreamSynchronize(st));
+    S->nseg = (S->chunks + SELL_SEG_CHUNKS - 1) / SELL_SEG_CHUNKS;
+    if ((rc = dmalloc((void **)&S->segrow, sizeof(int) * (S->nseg + 1)))) return fail(rc);
+    k_sell_segments<<<grid_of(s->ctx, S->nseg + 1), NT, 0, st>>>(S->choff, nh, S->nseg, S->segrow);
+    S->split = M.nnz >= SELL_SPLIT_NNZ;
     // rows too uneven for slices: more padding than the pass would save
     if (S->slots + 32 * S->chunks > SELL_MAX_SLOTS_PER_NNZ * std::max<int64_t>(M.nnz, 1024)) return fail(SP_OK);
     const int64_t hs = 32 * S->chunks;
@@ -632,14 +639,15 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
 
 void free_sell(SellMat *S, cudaStream_t st) {
     for (void *p : {(void *)S->ci, (void *)S->v, (void *)S->v32, (void *)S->off, (void *)S->slen, (void *)S->len,
-                    (void *)S->lsort, (void *)S->perm, (void *)S->heavy, (void *)S->choff, (void *)S->hci,
+                    (void *)S->lsort, (void *)S->perm, (void *)S->heavy, (void *)S->choff, (void *)S->segrow, (void *)S->hci,
                     (void *)S->hv, (void *)S->hv32})
         dfree(p, st);
     *S = SellMat{};
 }
 
-// A SELL pass: the warp rows on the solver's second stream, beside the windows on the
-// pass's stream (they write disjoint rows), joined before the next pass. Kernel shapes
+// A SELL pass: on a large pass the warp rows on the solver's second stream, beside the
+// windows on the pass's stream (they write disjoint rows), joined before the next pass; on a
+// small one both in one launch. Kernel shapes
 // from a sweep on the 40M LP (ms per pass, SELL path for both passes): warp rows with 2
 // chunks per batch at 4 CTAs/SM in FP64 (primal pass 0.276; 4 chunks at 3 CTAs/SM 0.290,
 // 4 or 8 at the registers' natural occupancy 0.288–0.293), 4 at 4 CTAs/SM in FP32 (0.255;
@@ -647,14 +655,21 @@ void free_sell(SellMat *S, cudaStream_t st) {
 // 0.193 FP64, 0.191 FP32; 4 entries 0.198, 8 at natural occupancy 0.207, 16 0.233).
 template <class Op>
 void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) {
-    const SellArgs a{S.ci,    S.v,   S.v32, S.off,  S.slen,  S.len,  S.lsort,  S.perm, S.heavy,
-                     S.choff, S.hci, S.hv,  S.hv32, S.nrows, S.nwin, S.nheavy, S.nseg};
+    const SellArgs a{S.ci,  S.v,     S.v32, S.off,  S.slen,  S.len,  S.lsort, S.perm,  S.heavy,
+                     S.choff, S.segrow, S.hci, S.hv, S.hv32, S.nrows, S.nwin, S.nheavy, S.nseg};
+    if (!S.split) {
+        const unsigned g = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32) + S.nwin);
+        if constexpr (sizeof(typename Op::VT) == 4) k_sell_both<Op, 4, 8, 1><<<g, NT, 0, st>>>(op, a);
+        else k_sell_both<Op, 2, 8, 1><<<g, NT, 0, st>>>(op, a);
+        return;
+    }
     const bool rows = S.nseg > 0;
     if (rows) {
         cudaEventRecord(s->fork, st);
         cudaStreamWaitEvent(s->aux, s->fork, 0);
         const unsigned gr = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32));
-        if constexpr (sizeof(typename Op::VT) == 4) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        // rows of 16+ chunks on average (the transport LP's 63): 4 chunks per batch
+        if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
         else k_sell_rows<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
     }
     k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
@@ -670,13 +685,19 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
 // in FP64 (0.255; tile engine 0.297, SELL 0.276 — 69 % of its nonzeros sit in warp rows)
 // and 4 in FP32 (0.247; SELL 0.255); the dual pass on its SELL copy in both precisions
 // (0.193 FP64, 0.191 FP32; tile engine 0.238 and 0.249, stream engine 0.300 and 0.227).
+// A problem under SMALL_NNZ nonzeros keeps both passes on the tile engine: there an
+// iteration's time is launch latency and tile parallelism (32 LPs of the batch workload,
+// one device solve each: 9.1 µs per iteration on tiles, 9.5 stream, 11.6 SELL).
 // SP_PASS_ENGINE=tiles|stream|sell overrides all four; SP_STREAM_GATHER names the
 // stream variant.
+constexpr int64_t SMALL_NNZ = 1 << 20;
+
 int choose_engines(sp_solver *s) {
-    s->sv_p64 = SV_LDG4_DEEP;
-    s->sv_p32 = SV_LDG4;
-    s->sv_d64 = ENGINE_SELL;
-    s->sv_d32 = ENGINE_SELL;
+    const bool small = s->nnz < SMALL_NNZ;
+    s->sv_p64 = small ? -1 : SV_LDG4_DEEP;
+    s->sv_p32 = small ? -1 : SV_LDG4;
+    s->sv_d64 = small ? -1 : ENGINE_SELL;
+    s->sv_d32 = small ? -1 : ENGINE_SELL;
     const char *eng = getenv("SP_PASS_ENGINE");
     if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
     if (eng && !strcmp(eng, "sell")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = ENGINE_SELL;
@@ -699,7 +720,7 @@ int choose_engines(sp_solver *s) {
         if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;
     for (int *v : {&s->sv_d64, &s->sv_d32})
         if (*v == ENGINE_SELL && !s->sellA.ok) *v = -1;
-    if ((s->sellA.ok || s->sellAT.ok) && !s->aux) {
+    if (((s->sellA.ok && s->sellA.split) || (s->sellAT.ok && s->sellAT.split)) && !s->aux) {
         SP_CUDA_TRY(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
         SP_CUDA_TRY(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
         SP_CUDA_TRY(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));

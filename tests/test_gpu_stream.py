@@ -110,6 +110,15 @@ def test_sell_path_equals_tile_engine(powerlaw_lp, gpu_backend):
                      solve_with("tiles", powerlaw_lp, params, gpu_backend))
 
 
+def test_sell_path_on_two_streams_equals_tile_engine(gpu_backend):
+    """A pass over 4M+ nonzeros runs its SELL warp rows and windows as two launches on two
+    streams (smaller passes in one launch): the same bits either way."""
+    lp = sp().generate_powerlaw_lp(3, 300_000, 600_000, 5_000_000, 1.5, 2, 1500)
+    for precision in (None, sp().Precision.Mixed):
+        params = fixed_iterations(192, precision)
+        assert_identical(solve_with("sell", lp, params, gpu_backend), solve_with("tiles", lp, params, gpu_backend))
+
+
 def test_sell_path_with_warp_rows_and_empty_rows(gpu_backend):
     # dense row of 1500 and dense column of 1800 entries (warp rows, no row beyond a tile),
     # empty rows and columns, ragged slices
