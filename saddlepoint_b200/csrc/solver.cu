@@ -149,43 +149,48 @@ __device__ __forceinline__ double inv_sqrt_d(double v) {  // scaling.rs:139-141
 }
 
 // Per-row geometric-mean factor 1/sqrt(min·max) of |a| (scaling.rs:62-63, min_max :159-178).
+// The row passes of the scaling below take each row with a group of G lanes (G = 4 … 32,
+// from the matrix's mean row length): min and max do not depend on the order, so the group
+// size changes no bit, and short rows no longer leave most of a warp idle. The row loop
+// steps a whole warp (32 / G rows) at a time so that every lane reaches each shuffle.
+template <int G>
 __global__ void k_row_geo(const int *rp, const double *v, int64_t rows, double *f) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, sub = lane % G;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = warp; r < rows; r += nw) {
+    for (int64_t base = warp * (32 / G); base < rows; base += nw * (32 / G)) {
+        const int64_t r = base + lane / G;
         double lo = INFINITY, hi = 0.0;
-        for (int k = rp[r] + lane; k < rp[r + 1]; k += 32) {
-            const double a = fabs(v[k]);
-            lo = fmin(lo, a);
-            hi = fmax(hi, a);
-        }
-        for (int o = 16; o; o >>= 1) {
+        if (r < rows)
+            for (int k = rp[r] + sub; k < rp[r + 1]; k += G) {
+                const double a = fabs(v[k]);
+                lo = fmin(lo, a);
+                hi = fmax(hi, a);
+            }
+        for (int o = G / 2; o; o >>= 1) {
             lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
             hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
         }
-        if (lane == 0) {
+        if (sub == 0 && r < rows) {
             if (hi == 0.0) lo = 0.0;
             f[r] = inv_sqrt_d(lo * hi);
         }
     }
 }
-
-// Per-row Ruiz factor 1/sqrt(max |a|) (scaling.rs:70-72).
+template <int G>
 __global__ void k_row_ruiz(const int *rp, const double *v, int64_t rows, double *f) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, sub = lane % G;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = warp; r < rows; r += nw) {
+    for (int64_t base = warp * (32 / G); base < rows; base += nw * (32 / G)) {
+        const int64_t r = base + lane / G;
         double hi = 0.0;
-        for (int k = rp[r] + lane; k < rp[r + 1]; k += 32) hi = fmax(hi, fabs(v[k]));
-        for (int o = 16; o; o >>= 1) hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        if (lane == 0) f[r] = inv_sqrt_d(hi);
+        if (r < rows)
+            for (int k = rp[r] + sub; k < rp[r + 1]; k += G) hi = fmax(hi, fabs(v[k]));
+        for (int o = G / 2; o; o >>= 1) hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        if (sub == 0 && r < rows) f[r] = inv_sqrt_d(hi);
     }
 }
-
-// Per-row Pock-Chambolle factor 1/sqrt(Σ|a|^α), summed in column order from 0.0
-// like abs_stats (scaling.rs:144-155), one thread per row.
 __global__ void k_row_pc(const int *rp, const double *v, int64_t rows, double alpha, double *f) {
     GRID_LOOP(r, rows) {
         double s = 0.0;
@@ -199,13 +204,14 @@ __global__ void k_row_pc(const int *rp, const double *v, int64_t rows, double al
 
 // values[k] *= r[i] * c[j] for every entry (i, j) (CsrMatrix::scale, problem.rs:120-126),
 // applied to A' (rows i) and, in the same pass over its own layout, to A'ᵀ.
+template <int G>
 __global__ void k_apply_rows(const int *rp, const int *ci, double *v, int64_t rows, const double *r, const double *c,
                              int transposed) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < rows; i += nw) {
-        for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
+    const int lane = threadIdx.x & 31, sub = lane % G;
+    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
+    for (int64_t i = grp; i < rows; i += ng) {
+        for (int k = rp[i] + sub; k < rp[i + 1]; k += G) {
             const int j = ci[k];
             // A'ᵀ row i is column i of A': the factor is still r[row] * c[col].
             const double f = transposed ? r[j] * c[i] : r[i] * c[j];
@@ -930,28 +936,46 @@ int scale_on_device(sp_solver *s, const sp_lp *lp) {
     int rc;
     if ((rc = dalloc(&r, m)) || (rc = dalloc(&c, n)) || (rc = dalloc(&ones_m, m)) || (rc = dalloc(&ones_n, n))) return rc;
     const int gm = grid_of(ctx, m), gn = grid_of(ctx, n);
-    const int wm = grid_of(ctx, m * 32), wn = grid_of(ctx, n * 32);
+    // lanes per row of the row passes: about half the mean row length, 4 to 32
+    auto group_of = [](int64_t z, int64_t rows) {
+        const int64_t half = rows > 0 ? (z / rows + 1) / 2 : 1;
+        int g = 4;
+        while (g < 32 && g < half) g *= 2;
+        return g;
+    };
+    const int Gm = group_of(nnz, m), Gn = group_of(nnz, n);
+    const int wm = grid_of(ctx, m * Gm), wn = grid_of(ctx, n * Gn);
+    // K<G><<<...>>>(args) for the group size g
+#define SP_ROW_LAUNCH(K, g, grid, ...)                                     \
+    do {                                                                  \
+        switch (g) {                                                      \
+        case 4: K<4><<<grid, NT, 0, st>>>(__VA_ARGS__); break;            \
+        case 8: K<8><<<grid, NT, 0, st>>>(__VA_ARGS__); break;            \
+        case 16: K<16><<<grid, NT, 0, st>>>(__VA_ARGS__); break;          \
+        default: K<32><<<grid, NT, 0, st>>>(__VA_ARGS__); break;          \
+        }                                                                 \
+    } while (0)
     k_fill<<<gm, NT, 0, st>>>(ones_m, 1.0, m);
     k_fill<<<gn, NT, 0, st>>>(ones_n, 1.0, n);
     k_fill<<<gm, NT, 0, st>>>(s->row_scale, 1.0, m);
     k_fill<<<gn, NT, 0, st>>>(s->col_scale, 1.0, n);
     auto apply = [&](const double *rr, const double *cc) {  // apply (scaling.rs:180-184)
         if (nnz) {
-            k_apply_rows<<<wm, NT, 0, st>>>(s->A.rp, s->A.ci, s->A.v, m, rr, cc, 0);
-            k_apply_rows<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.ci, s->AT.v, n, rr, cc, 1);
+            SP_ROW_LAUNCH(k_apply_rows, Gm, wm, s->A.rp, s->A.ci, s->A.v, m, rr, cc, 0);
+            SP_ROW_LAUNCH(k_apply_rows, Gn, wn, s->AT.rp, s->AT.ci, s->AT.v, n, rr, cc, 1);
         }
         k_mul_inplace<<<gm, NT, 0, st>>>(s->row_scale, rr, m);
         k_mul_inplace<<<gn, NT, 0, st>>>(s->col_scale, cc, n);
     };
     for (uint64_t pass = 0; pass < P.geometric_mean_passes; ++pass) {
-        k_row_geo<<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, r);
+        SP_ROW_LAUNCH(k_row_geo, Gm, wm, s->A.rp, s->A.v, m, r);
         apply(r, ones_n);
-        k_row_geo<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, c);
+        SP_ROW_LAUNCH(k_row_geo, Gn, wn, s->AT.rp, s->AT.v, n, c);
         apply(ones_m, c);
     }
     for (uint64_t it = 0; it < P.ruiz_iterations; ++it) {
-        k_row_ruiz<<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, r);
-        k_row_ruiz<<<wn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, c);
+        SP_ROW_LAUNCH(k_row_ruiz, Gm, wm, s->A.rp, s->A.v, m, r);
+        SP_ROW_LAUNCH(k_row_ruiz, Gn, wn, s->AT.rp, s->AT.v, n, c);
         apply(r, c);
     }
     if (P.pock_chambolle_enabled) {
@@ -976,6 +1000,7 @@ int scale_on_device(sp_solver *s, const sp_lp *lp) {
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     for (double *b : {r, c, ones_m, ones_n, oc, olc, ouc, olv, ouv}) dfree(b, st);
     return SP_OK;
+#undef SP_ROW_LAUNCH
 }
 
 // A'ᵀ on the device: a stable radix sort of the column indices (cub) gives, per
