@@ -39,7 +39,9 @@ constexpr uint8_t SELL_HEAVY = 0xFF;           // length mark of a warp row
 constexpr int SELL_WIN_SHIFT = 10;
 constexpr int SELL_WIN = 1 << SELL_WIN_SHIFT;        // rows per window: one CTA's work
 constexpr int SELL_SPW = SELL_WIN / 32 / (NT / 32);  // slices per warp in a window
-constexpr int SELL_SEG_CHUNKS = 32;  // chunks per block: a warp takes the rows starting in one (primal pass of the 40M LP: 8 0.316 ms, 16 0.279, 32 0.267, 48 0.268, 62 0.270)
+// Chunks per block: a warp takes the rows starting in one (the 40M LP's primal pass on this
+// path, ms: blocks of 8 0.316, 16 0.279, 32 0.267, 48 0.268, 62 0.270).
+constexpr int SELL_SEG_CHUNKS = 32;
 static_assert(SELL_WIN % NT == 0 && SELL_SPW >= 1, "a window is a whole number of slices per warp");
 static_assert(SELL_SEG_CHUNKS / 2 < 32, "a segment's row bounds sit in one lane each");
 

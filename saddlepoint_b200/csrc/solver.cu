@@ -645,8 +645,8 @@ int build_sell(sp_solver *s, const DevCsr &M, SellMat *S) {
 
 void free_sell(SellMat *S, cudaStream_t st) {
     for (void *p : {(void *)S->ci, (void *)S->v, (void *)S->v32, (void *)S->off, (void *)S->slen, (void *)S->len,
-                    (void *)S->lsort, (void *)S->perm, (void *)S->heavy, (void *)S->choff, (void *)S->segrow, (void *)S->hci,
-                    (void *)S->hv, (void *)S->hv32})
+                    (void *)S->lsort, (void *)S->perm, (void *)S->heavy, (void *)S->choff, (void *)S->segrow,
+                    (void *)S->hci, (void *)S->hv, (void *)S->hv32})
         dfree(p, st);
     *S = SellMat{};
 }
