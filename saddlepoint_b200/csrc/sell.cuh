@@ -369,3 +369,208 @@ __global__ void __launch_bounds__(NT, MINB) k_sell_both(Op op, SellArgs S) {
 }
 
 }  // namespace sp
+
+namespace sp {
+
+// ---- check passes on the SELL copy -------------------------------------------------
+//
+// A pass with G product slots and NP partial sums across rows (the check iteration's dual
+// pass) runs on the SELL copy in two launches. k_sell_chk sums every row's G slots exactly
+// as the tile engine does (the same order per slot, the same tree for a warp row) and runs
+// its epilogue with partial sums that start at zero, storing each row's NP contributions
+// in `contrib` ([NP][nrows]). k_sell_refold then adds them up per tile in the tile
+// engine's order — each thread its short rows, lane 0 of warp w the warp rows w, w + 8, …,
+// then the block tree — and stores the tile's partials. A partial sum never becomes -0.0,
+// so adding a contribution that started from +0.0 gives the bits the tile engine's
+// in-place accumulation gives.
+
+template <int G, unsigned F32>
+struct SlotSums {
+    float f[G];
+    double d[G];
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int q = 0; q < G; ++q) { f[q] = -0.0f; d[q] = -0.0; }
+    }
+    template <class ST>
+    __device__ __forceinline__ void add(const ST (&p)[G]) {
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            if ((F32 >> q) & 1u) f[q] += float(p[q]);
+            else d[q] += double(p[q]);
+        }
+    }
+    __device__ __forceinline__ double get(int q) const { return ((F32 >> q) & 1u) ? double(f[q]) : d[q]; }
+};
+
+// One row's epilogue with its partials from zero, stored as its contributions.
+template <class Op>
+__device__ __forceinline__ void row_contrib(const Op &op, int r, const double (&sum)[Op::G],
+                                            const typename Op::Pre &pre, double *contrib, int64_t nrows) {
+    double part[Op::NP];
+#pragma unroll
+    for (int q = 0; q < Op::NP; ++q) part[q] = 0.0;
+    op.row(r, sum, part, pre);
+#pragma unroll
+    for (int q = 0; q < Op::NP; ++q) contrib[q * nrows + r] = part[q];
+}
+
+// Segments (warp rows) first, one per warp, BH chunks per batch; then the windows.
+template <class Op, int BH, int BS>
+__global__ void __launch_bounds__(NT) k_sell_chk(Op op, SellArgs S, double *contrib) {
+    using VT = typename Op::VT;
+    using ST = typename Op::ST;
+    using Pre = typename Op::Pre;
+    constexpr int G = Op::G;
+    constexpr unsigned F32 = Op::F32;
+    constexpr int W = NT / 32;
+    __shared__ double sums[G * SELL_WIN];
+    if (!op.setup()) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t hb = (S.nseg + W - 1) / W;
+    const VT *__restrict__ hv;
+    const VT *__restrict__ sv;
+    if constexpr (sizeof(VT) == 4) {
+        hv = reinterpret_cast<const VT *>(S.hv32);
+        sv = reinterpret_cast<const VT *>(S.v32);
+    } else {
+        hv = reinterpret_cast<const VT *>(S.hv);
+        sv = reinterpret_cast<const VT *>(S.v);
+    }
+    if ((int64_t)blockIdx.x < hb) {
+        const int64_t seg = (int64_t)blockIdx.x * W + warp;
+        if (seg >= S.nseg) return;
+        const int64_t h0 = S.segrow[seg];
+        const int nr = S.segrow[seg + 1] - (int)h0;
+        if (nr == 0) return;
+        int row = 0;
+        int64_t bound = 0;
+        Pre pre{};
+        if (lane <= nr) bound = S.choff[h0 + lane];
+        if (lane < nr) {
+            row = S.heavy[h0 + lane];
+            pre = op.pre(row);
+        }
+        const int64_t c0 = __shfl_sync(0xffffffffu, bound, 0), c1 = __shfl_sync(0xffffffffu, bound, nr);
+        const int nch = (int)(c1 - c0);
+        int cur = 0, nxt = (int)(__shfl_sync(0xffffffffu, bound, 1) - c0);
+        SlotSums<G, F32> acc;
+        acc.clear();
+        auto finish = [&]() {
+            double tot[G];
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                if ((F32 >> q) & 1u) tot[q] = double(__shfl_sync(0xffffffffu, warp_sum_down(acc.f[q]), 0));
+                else tot[q] = __shfl_sync(0xffffffffu, warp_sum_down(acc.d[q]), 0);
+            }
+            if (lane == cur) row_contrib(op, row, tot, pre, contrib, S.nrows);
+        };
+        for (int ch = 0; ch < nch; ch += BH) {
+            int c[BH];
+            VT v[BH];
+            ST p[BH][G];
+#pragma unroll
+            for (int u = 0; u < BH; ++u) {
+                c[u] = -1;
+                if (ch + u < nch) {
+                    c[u] = ld_stream(S.hci + (c0 + ch + u) * 32 + lane);
+                    v[u] = ld_stream(hv + (c0 + ch + u) * 32 + lane);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BH; ++u)
+                if (c[u] >= 0) op.prod(c[u], v[u], p[u]);
+#pragma unroll
+            for (int u = 0; u < BH; ++u) {
+                if (ch + u >= nch) break;
+                if (ch + u == nxt) {  // a warp row spans at least two chunks
+                    finish();
+                    ++cur;
+                    nxt = (int)(__shfl_sync(0xffffffffu, bound, cur + 1) - c0);
+                    acc.clear();
+                }
+                if (c[u] >= 0) acc.add(p[u]);
+            }
+        }
+        finish();
+        return;
+    }
+    const int64_t win = blockIdx.x - hb;
+#pragma unroll 1
+    for (int qs = 0; qs < SELL_SPW; ++qs) {
+        const int ls = qs * W + ((qs & 1) ? W - 1 - warp : warp);
+        const int64_t sl = win * (SELL_WIN / 32) + ls;
+        const int64_t k = sl * 32 + lane;
+        const int l = S.lsort[k];
+        const int L = S.slen[sl];
+        const int64_t off = S.off[sl] + lane;
+        SlotSums<G, F32> acc;
+        acc.clear();
+        for (int j0 = 0; j0 < L; j0 += BS) {
+            int c[BS];
+            VT v[BS];
+            ST p[BS][G];
+#pragma unroll
+            for (int u = 0; u < BS; ++u) {
+                if (j0 + u < l) {
+                    c[u] = ld_stream(S.ci + off + 32ll * (j0 + u));
+                    v[u] = ld_stream(sv + off + 32ll * (j0 + u));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < BS; ++u)
+                if (j0 + u < l) op.prod(c[u], v[u], p[u]);
+#pragma unroll
+            for (int u = 0; u < BS; ++u)
+                if (j0 + u < l) acc.add(p[u]);
+        }
+        const int at = S.perm[k];
+#pragma unroll
+        for (int q = 0; q < G; ++q) sums[q * SELL_WIN + at] = acc.get(q);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < SELL_WIN; t += NT) {
+        const int64_t r = win * SELL_WIN + t;
+        if (r >= S.nrows) break;
+        if (S.len[r] == SELL_HEAVY) continue;
+        double tot[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) tot[q] = sums[q * SELL_WIN + t];
+        row_contrib(op, (int)r, tot, op.pre((int)r), contrib, S.nrows);
+    }
+}
+
+// The tile partials of a k_sell_chk pass from its contributions, one CTA per tile (the
+// matrix has no tile of a single row longer than TILE_NNZ: it has a SELL copy).
+template <class Op>
+__global__ void __launch_bounds__(NT) k_sell_refold(Op op, const uint8_t *__restrict__ len,
+                                                    const double *__restrict__ contrib, int64_t nrows) {
+    constexpr int NP = Op::NP;
+    __shared__ double sh[NP * (NT / 32)];
+    if (!op.setup()) return;
+    const int tile = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Tile t = op.tiles[tile];
+    const int r0 = t.x, nr = t.y - t.x;
+    double part[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) part[q] = 0.0;
+    auto add = [&](int64_t r) {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) part[q] += contrib[q * nrows + r];
+    };
+    // short rows: thread u takes rows u, u + NT, …
+    for (int u = tid; u < nr; u += NT)
+        if (len[r0 + u] != SELL_HEAVY) add(r0 + u);
+    // warp rows: warp w the rows w, w + 8, … in increasing order, on lane 0
+    for (int base = warp; base < nr; base += 32 * (NT / 32)) {
+        const int i = base + lane * (NT / 32);
+        const bool heavy = i < nr && len[r0 + i] == SELL_HEAVY;
+        for (unsigned mask = __ballot_sync(0xffffffffu, heavy); mask; mask &= mask - 1)
+            if (lane == 0) add(r0 + base + (__ffs(mask) - 1) * (NT / 32));
+    }
+    __syncthreads();
+    block_sum<NP>(part, sh);
+    if (tid == 0) op.store(tile, part);
+}
+
+}  // namespace sp

@@ -651,6 +651,21 @@ void free_sell(SellMat *S, cudaStream_t st) {
     *S = SellMat{};
 }
 
+SellArgs sell_args(const SellMat &S) {
+    return SellArgs{S.ci,     S.v,   S.v32, S.off,  S.slen,  S.len,  S.lsort,  S.perm, S.heavy,
+                    S.choff,  S.segrow, S.hci, S.hv, S.hv32, S.nrows, S.nwin, S.nheavy, S.nseg};
+}
+
+// A check pass on the SELL copy: rows' contributions, then the tile partials from them
+// (sell.cuh: k_sell_chk, k_sell_refold). The same bits as the tile engine's pass.
+template <class Op>
+void launch_sell_check(sp_solver *s, const SellMat &S, const DevCsr &M, cudaStream_t st, const Op &op) {
+    const SellArgs a = sell_args(S);
+    const unsigned g = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32) + S.nwin);
+    k_sell_chk<Op, 2, 4><<<g, NT, 0, st>>>(op, a, s->contrib);
+    k_sell_refold<Op><<<M.ntiles, NT, 0, st>>>(op, S.len, s->contrib, S.nrows);
+}
+
 // A SELL pass: on a large pass the warp rows on the solver's second stream, beside the
 // windows on the pass's stream (they write disjoint rows), joined before the next pass; on a
 // small one both in one launch. Kernel shapes from a sweep on the 40M LP (ms per pass, SELL
@@ -662,8 +677,7 @@ void free_sell(SellMat *S, cudaStream_t st) {
 // chunks per batch: dual pass 0.053 ms (2 chunks 0.060, 8 0.060).
 template <class Op>
 void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) {
-    const SellArgs a{S.ci,  S.v,     S.v32, S.off,  S.slen,  S.len,  S.lsort, S.perm,  S.heavy,
-                     S.choff, S.segrow, S.hci, S.hv, S.hv32, S.nrows, S.nwin, S.nheavy, S.nseg};
+    const SellArgs a = sell_args(S);
     if (!S.split) {
         const unsigned g = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32) + S.nwin);
         if constexpr (sizeof(typename Op::VT) == 4) k_sell_both<Op, 4, 8, 1><<<g, NT, 0, st>>>(op, a);
@@ -727,6 +741,10 @@ int choose_engines(sp_solver *s) {
         if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;
     for (int *v : {&s->sv_d64, &s->sv_d32})
         if (*v == ENGINE_SELL && !s->sellA.ok) *v = -1;
+    // the check's dual pass on the SELL copy too, where the iteration's dual pass uses it
+    if (s->sellA.ok && s->sv_d64 == ENGINE_SELL && !s->contrib &&
+        (rc = dmalloc((void **)&s->contrib, sizeof(double) * NP_D * std::max<int64_t>(s->A.nrows, 1))))
+        return rc;
     if (((s->sellA.ok && s->sellA.split) || (s->sellAT.ok && s->sellAT.split)) && !s->aux) {
         SP_CUDA_TRY(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
         SP_CUDA_TRY(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
@@ -785,6 +803,11 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
     const int g = s->A.ntiles;
     if (g == 0) return;
     const size_t sm = smem_D();
+    if (role == ROLE_CHECK && s->contrib) {
+        if (s->mixed) launch_sell_check(s, s->sellA, s->A, st, mkD<true, 2>(p, i, role));
+        launch_sell_check(s, s->sellA, s->A, st, mkD<false, 2>(p, i, role));
+        return;
+    }
     if (role == ROLE_MID && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
         const size_t s1 = tile_smem_bytes<1, double>();
         if (s->mixed) {
@@ -917,6 +940,7 @@ void solver_release(sp_solver *s) {
     free_sell(&s->sellAT, fst);
     void *bufs[] = {s->c, s->lc, s->uc, s->lv, s->uv, s->pf, s->df, s->x, s->y, s->xt, s->yt, s->xbar, s->xa, s->ya,
                     s->aty, s->xbar32, s->y32, s->pk, s->pky, s->partP, s->partD, s->partT, s->partP0, s->partD0, s->pv, s->ptmp,
+                    s->contrib,
                     s->ppart, s->row_scale, s->col_scale, s->scales, s->d_prm, s->d_st, s->d_trace, s->norms,
                     s->out_x, s->out_y};
     for (void *b : bufs) dfree(b, fst);

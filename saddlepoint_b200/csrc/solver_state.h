@@ -24,6 +24,7 @@ struct sp_solver {
     sp::SellMat sellA, sellAT;  // SELL copies of A' (dual pass) and A'ᵀ (primal pass), when used
     cudaStream_t aux = nullptr;  // second stream of a SELL pass: its warp rows beside its windows
     cudaEvent_t fork = nullptr, join = nullptr;
+    double *contrib = nullptr;   // [NP_D][m] row contributions of the check's dual pass on the SELL copy
     int64_t m = 0, n = 0, nnz = 0;
     double c0 = 0.0;
     int maximize = 0;
