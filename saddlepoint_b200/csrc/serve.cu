@@ -22,6 +22,7 @@
 #include <thread>
 #include <vector>
 
+#include "control.cuh"
 #include "internal.cuh"
 
 namespace {
@@ -187,10 +188,11 @@ extern "C" int64_t sp_server_footprint(int64_t m, int64_t n, int64_t nnz, int pr
     // the transpose's sort buffers at set-up (about 24 bytes per nonzero), the SELL
     // copy of A' (at most two slots per nonzero, 12 or 16 bytes each, and at most 18 bytes
     // per row for its lengths, order, warp-row list, chunk and slice offsets, the last
-    // window padded), the n- and m-vectors of the solve, and 8 MiB of fixed overhead.
+    // window padded, plus the check's 64 bytes of row contributions), the n- and m-vectors
+    // of the solve, and 8 MiB of fixed overhead.
     int64_t b = 2 * nnz * 12 + 24 * nnz + 4 * (m + n + 2);
     if (precision == SP_PRECISION_MIXED) b += 2 * nnz * 4 + 4 * (m + n);
-    b += 2 * nnz * (precision == SP_PRECISION_MIXED ? 16 : 12) + 18 * (m + 1024) + 2 * 1024 * 16;
+    b += 2 * nnz * (precision == SP_PRECISION_MIXED ? 16 : 12) + (18 + 8 * sp::NP_D) * (m + 1024) + 2 * 1024 * 16;
     b += 168 * n + 120 * m + (8ll << 20);
     return b;
 }
