@@ -347,6 +347,16 @@ void sp_lp_release(sp_lp *lp);
  * message in err (any of the two may be null). Row and column names are not kept. */
 int sp_read_mps(const char *text, size_t len, sp_lp *out, int64_t *err_line, char *err, size_t errlen);
 
+/* CsrMatrix::from_triplets (crates/saddlepoint-core/src/problem.rs:33-77) on the GPU of
+ * `ctx`, for loading large problems: ntrip (row, column, value) triplets in host memory to
+ * a CSR matrix with library-owned host arrays (release with sp_csr_release). Entries are
+ * grouped by row, ordered by column within a row, runs of one column summed in input order
+ * and exact-zero sums dropped: bit for bit the host rule (and sp_read_mps's). An index out
+ * of range returns SP_ERR_INVALID (the reference asserts). */
+int sp_csr_from_triplets(sp_ctx *ctx, int64_t nrows, int64_t ncols, int64_t ntrip, const int64_t *rows,
+                         const int64_t *cols, const double *vals, sp_csr *out);
+void sp_csr_release(sp_csr *m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,7 @@ __all__ = [
     "BackendError", "SolveError", "Status", "Termination", "Precision", "LpProblem", "ScaledProblem",
     "SolverParams", "Solution", "CudaBackend", "Solver", "solve", "solve_stepwise", "BatchSolver", "Server",
     "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library", "read_mps", "MpsError",
+    "csr_from_triplets",
 ]
 
 
@@ -580,6 +581,30 @@ def read_mps(source, name: str = "") -> LpProblem:
     if rc != L.SP_OK:
         raise BackendError(rc, "sp_read_mps failed")
     return _take_lp(out, name)
+
+
+def csr_from_triplets(nrows: int, ncols: int, rows, cols, vals, backend: "CudaBackend"):
+    """CsrMatrix::from_triplets (crates/saddlepoint-core/src/problem.rs:33-77) on the GPU:
+    (row_ptr int64, col_idx int32, values float64) of the CSR matrix, bit for bit the host
+    rule (runs of one (row, column) summed in input order, exact-zero sums dropped). An
+    index out of range raises BackendError (the reference asserts)."""
+    r = np.ascontiguousarray(rows, dtype=np.int64)
+    c = np.ascontiguousarray(cols, dtype=np.int64)
+    v = np.ascontiguousarray(vals, dtype=np.float64)
+    if not (len(r) == len(c) == len(v)):
+        raise ValueError("rows, cols and vals differ in length")
+    out = L.Csr()
+    pi = lambda a: a.ctypes.data_as(L.PI64)  # noqa: E731
+    backend._check(backend.lib.sp_csr_from_triplets(backend.h, nrows, ncols, len(v), pi(r), pi(c),
+                                                    v.ctypes.data_as(L.PD), C.byref(out)))
+    nnz = out.nnz
+
+    def arr(ptr, k, dt):
+        return np.ctypeslib.as_array(ptr, shape=(k,)).astype(dt, copy=True) if k else np.zeros(0, dt)
+
+    res = (arr(out.row_ptr, nrows + 1, np.int64), arr(out.col_idx, nnz, np.int32), arr(out.values, nnz, np.float64))
+    backend.lib.sp_csr_release(C.byref(out))
+    return res
 
 
 # ------------------------------------------------------------------ generators
