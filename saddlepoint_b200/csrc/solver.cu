@@ -766,7 +766,9 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     const int g = s->AT.ntiles;
     if (g == 0) return;
     const size_t sm = smem_P();
-    if (role == ROLE_MID && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
+    // MID passes, and the FUSED variant of an epoch's first pass (it returns at once when the
+    // epoch opens at k = 0), on the pass's engine; the first pass's k = 0 variant on tiles
+    if ((role == ROLE_MID || role == ROLE_FIRST) && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
         if (s->mixed) {
             if (s->sv_p32 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<true, 0>(p, i, role));
             else if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
@@ -775,6 +777,10 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
         if (s->sv_p64 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<false, 0>(p, i, role));
         else if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
         else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 0>(p, i, role));
+        if (role == ROLE_FIRST) {
+            if (s->mixed) launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 1>(p, i, role), mkP<false, 1>(p, i, role));
+            else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 1>(p, i, role));
+        }
         return;
     }
     if (s->mixed) {
@@ -808,7 +814,7 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
         launch_sell_check(s, s->sellA, s->A, st, mkD<false, 2>(p, i, role));
         return;
     }
-    if (role == ROLE_MID && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
+    if ((role == ROLE_MID || role == ROLE_FIRST) && (s->sv_d64 >= 0 || (s->mixed && s->sv_d32 >= 0))) {
         const size_t s1 = tile_smem_bytes<1, double>();
         if (s->mixed) {
             if (s->sv_d32 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<true, 0>(p, i, role));
@@ -818,6 +824,18 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
         if (s->sv_d64 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<false, 0>(p, i, role));
         else if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
         else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, s1, st, mkD<false, 0>(p, i, role));
+        if (role == ROLE_FIRST) {
+            // the k = 0 variant: two products and two partial sums per row
+            if (s->contrib) {
+                if (s->mixed) launch_sell_check(s, s->sellA, s->A, st, mkD<true, 1>(p, i, role));
+                launch_sell_check(s, s->sellA, s->A, st, mkD<false, 1>(p, i, role));
+            } else if (s->mixed) {
+                launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<2, double>(), st, mkD<true, 1>(p, i, role),
+                             mkD<false, 1>(p, i, role));
+            } else {
+                launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, tile_smem_bytes<2, double>(), st, mkD<false, 1>(p, i, role));
+            }
+        }
         return;
     }
     if (s->mixed) {
