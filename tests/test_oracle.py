@@ -187,6 +187,37 @@ def test_from_triplets_sums_duplicates_and_drops_zeros():
     assert list(v) == [5.0, 5.0, 4.0]
 
 
+def test_from_triplets_sums_each_pair_in_input_order():
+    """The stated rule for repeated (row, column) pairs (problem.rs sorts each row with
+    sort_unstable_by_key, which leaves their order open): a stable sort, so each pair's
+    values are summed in input order — the rule the GPU builder (sp_csr_from_triplets) is
+    held to. Checked against a plain restatement on random triplets with many repeats."""
+    rng = np.random.default_rng(3)
+    for trial in range(20):
+        m, n, k = int(rng.integers(1, 30)), int(rng.integers(1, 12)), int(rng.integers(0, 400))
+        rows = rng.integers(0, m, k)
+        cols = rng.integers(0, n, k)
+        vals = rng.choice([1e16, -1e16, 1.0, -1.0, 0.5, -0.0, 0.0, 3.25], k)
+        want_rp, want_ci, want_v = [0], [], []
+        for i in range(m):
+            entries = sorted([(int(c), t) for t, (r, c) in enumerate(zip(rows, cols)) if r == i])
+            j = 0
+            while j < len(entries):
+                c, t = entries[j]
+                total = vals[t]
+                j += 1
+                while j < len(entries) and entries[j][0] == c:
+                    total = total + vals[entries[j][1]]
+                    j += 1
+                if total != 0.0:
+                    want_ci.append(c)
+                    want_v.append(total)
+            want_rp.append(len(want_ci))
+        rp, ci, v = oracle.from_triplets(m, n, rows, cols, vals)
+        assert list(rp) == want_rp and list(ci) == want_ci
+        assert np.array_equal(np.asarray(v, dtype=np.float64).view(np.uint64), np.asarray(want_v, dtype=np.float64).view(np.uint64))
+
+
 def test_transpose_is_stable_counting_sort():
     rp, ci, v = oracle.from_triplets(3, 3, [0, 0, 1, 2, 2], [0, 2, 2, 0, 1], [1.0, 2.0, 3.0, 4.0, 5.0])
     trp, tci, tv = oracle.transpose(3, 3, rp, ci, v)
