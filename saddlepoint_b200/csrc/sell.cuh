@@ -36,8 +36,10 @@ namespace sp {
 
 constexpr int64_t SELL_MAX_SLOTS_PER_NNZ = 2;  // padding cap of a SELL copy (server footprints count it)
 constexpr uint8_t SELL_HEAVY = 0xFF;           // length mark of a warp row
-constexpr int SELL_WIN_SHIFT = 10;
-constexpr int SELL_WIN = 1 << SELL_WIN_SHIFT;        // rows per window: one CTA's work
+constexpr int SELL_WIN_SHIFT = 9;
+// Rows per window: one CTA's work (the 40M LP's dual pass, ms FP64 / FP32: 256 rows 0.197 /
+// 0.182, 512 0.188 / 0.182, 1,024 0.193 / 0.190).
+constexpr int SELL_WIN = 1 << SELL_WIN_SHIFT;
 constexpr int SELL_SPW = SELL_WIN / 32 / (NT / 32);  // slices per warp in a window
 // Chunks per block: a warp takes the rows starting in one (the 40M LP's primal pass on this
 // path, ms: blocks of 8 0.316, 16 0.279, 32 0.267, 48 0.268, 62 0.270).
