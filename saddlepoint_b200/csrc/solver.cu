@@ -672,7 +672,7 @@ void launch_sell_check(sp_solver *s, const SellMat &S, const DevCsr &M, cudaStre
 // path for both passes, 16-row segments): warp rows with 2 chunks per batch at 4 CTAs/SM in
 // FP64 (primal pass 0.276; 4 chunks at 3 CTAs/SM 0.290, 4 or 8 at the registers' natural
 // occupancy 0.288–0.293), 4 at 4 CTAs/SM in FP32 (0.255; 2 chunks 0.264); windows with 8
-// slice entries in flight at 4 CTAs/SM in both (dual pass 0.193 FP64, 0.191 FP32; 4 entries
+// slice entries in flight at 4 CTAs/SM in both (1,024-row windows: dual pass 0.193 FP64, 0.191 FP32; 4 entries
 // 0.198, 8 at natural occupancy 0.207, 16 0.233). On the transport LP's 63-chunk rows, 4
 // chunks per batch: dual pass 0.053 ms (2 chunks 0.060, 8 0.060).
 template <class Op>
@@ -705,7 +705,8 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
 // per launch): the primal pass on the stream engine with 4 register-gatherer warps, 4 slots
 // in FP64 (0.255; tile engine 0.297, SELL 0.267 — 69 % of its nonzeros sit in warp rows)
 // and 4 in FP32 (0.247; SELL 0.255); the dual pass on its SELL copy in both precisions
-// (0.193 FP64, 0.191 FP32; tile engine 0.238 and 0.249, stream engine 0.300 and 0.227).
+// (0.185 FP64, 0.182 FP32 with 512-row windows; tile engine 0.238 and 0.249, stream engine
+// 0.300 and 0.227).
 // A problem under SMALL_NNZ nonzeros keeps both passes on the tile engine: there an
 // iteration's time is launch latency and tile parallelism (32 LPs of the batch workload,
 // one device solve each: 9.1 µs per iteration on tiles, 9.5 stream, 11.6 SELL).
