@@ -693,7 +693,9 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
         if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
         else k_sell_rows<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
     }
-    k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    // FP32 values: 5 CTAs per SM (0.176 ms against 0.182 at 4, with 512-row windows)
+    if constexpr (sizeof(typename Op::VT) == 4) k_sell_win<Op, 8, 5><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    else k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
     if (rows) {
         cudaEventRecord(s->join, s->aux);
         cudaStreamWaitEvent(st, s->join, 0);
