@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the power-law LP's m, n and nnz by this factor (profiling runs only)")
+    ap.add_argument("--tolerance", type=float, default=1e-6, help="relative KKT target of the to-tolerance solves")
+    ap.add_argument("--tolerance-limit-s", type=float, default=120.0, help="time limit of each to-tolerance solve")
+    ap.add_argument("--no-tolerance", action="store_true", help="skip the solves to the tolerance")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-form section of the default line")
     return ap.parse_args()
 
 
@@ -156,15 +160,16 @@ def measured_peak():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present
-    (a line 'dram_bytes_per_launch <kernel> <bytes>' in profiles/ncu_traffic.txt)."""
+def profiled_traffic(kernel: str, workload: str, form: str):
+    """DRAM bytes per launch of `kernel` on this exact workload and form, from the committed
+    ncu summary (a line 'dram_bytes_per_launch <kernel> <workload> <form> <bytes>' in
+    profiles/ncu_traffic.txt); None when no capture covers it."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     try:
         for line in open(path):
             f = line.split()
-            if len(f) >= 3 and f[0] == "dram_bytes_per_launch" and f[1] == kernel:
-                return float(f[2])
+            if len(f) >= 5 and f[0] == "dram_bytes_per_launch" and f[1:4] == [kernel, workload, form]:
+                return float(f[4])
     except OSError:
         pass
     return None
@@ -172,11 +177,26 @@ def profiled_traffic(kernel: str):
 
 # ------------------------------------------------------------------ workloads
 
+POWERLAW = (2_000_000, 4_000_000, 40_000_000)
+
+
+def powerlaw_shape(scale: float = 1.0):
+    return tuple(int(round(v * scale)) for v in POWERLAW)
+
+
 def powerlaw_lp(seed: int, scale: float = 1.0):
     import saddlepoint_b200 as sp
 
-    m, n, nnz = (int(round(v * scale)) for v in (2_000_000, 4_000_000, 40_000_000))
+    m, n, nnz = powerlaw_shape(scale)
     return sp.generate_powerlaw_lp(seed, m, n, nnz, 1.5, 2, 5000)
+
+
+def workload_key(workload: str, scale: float = 1.0) -> str:
+    """The name a profile capture is filed under: the workload at its full-launch size."""
+    if workload == "powerlaw":
+        m, n, nnz = powerlaw_shape(scale)
+        return f"powerlaw_m{m}_n{n}_nnz{nnz}"
+    return "transport_2000x2000"
 
 
 WORKLOAD_DESC = {
@@ -188,9 +208,31 @@ WORKLOAD_DESC = {
 }
 
 
+def workload_config(args):
+    cfg = dict(WORKLOAD_DESC[args.workload], seed=args.seed)
+    if args.scale != 1.0:
+        m, n, nnz = powerlaw_shape(args.scale)
+        cfg.update(scale=args.scale, m=m, n=n, nnz=nnz)
+    return cfg
+
+
+GOLDEN_FULL = os.path.join(ROOT, "tests", "golden", "powerlaw_m2000000_n4000000_nnz40000000_seed1.json")
+
+
+def oracle_golden(args):
+    """The oracle's committed FP64 solve of the default workload at 1e-6 (status, iterations,
+    objective), written by tests/golden/make_scale_goldens.py; None for other workloads."""
+    if args.workload != "powerlaw" or args.scale != 1.0 or args.seed != 1:
+        return None
+    try:
+        with open(GOLDEN_FULL) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
 def pinned_copy(lp):
     """The LP's arrays in page-locked host memory (the e2e inputs)."""
-    import numpy as np
     import torch
 
     import saddlepoint_b200 as sp
@@ -214,14 +256,15 @@ def pinned_copy(lp):
 
 
 def time_form(sp, torch, lp, backend, precision, steps, warmup, dist, device):
-    """Device-resident iterations/s of one precision; returns a dict of measurements."""
-    # tolerances of 0: no check ever ends the solve, every timed epoch runs its 64 iterations
+    """Device-resident iterations/s of one precision on the product's path (each epoch one
+    CUDA-graph replay), then per-pass launch times from CUDA events in a separate,
+    untimed pass of direct launches; returns a dict of measurements."""
+    # tolerances of 0: no check ends the solve, every timed epoch runs its 64 iterations
     params = sp.SolverParams(tolerance=0.0, infeasibility_tolerance=0.0, max_iterations=10**9, precision=precision)
     solver = sp.Solver(lp, params, backend)
     stream = torch.cuda.ExternalStream(backend.stream(), device=f"cuda:{device}")
     solver.run_epochs(warmup)
     solver.sync()
-    solver.set_timing(4)  # events around every 4th primal/dual launch pair
     dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(device)
@@ -236,23 +279,55 @@ def time_form(sp, torch, lp, backend, precision, steps, warmup, dist, device):
     done = solver.info().iterations
     if done != (warmup + steps) * ITERS_PER_STEP:
         raise RuntimeError(f"the timed solve stopped early: {done} iterations, status {solver.info().status}")
+    # launch times of the two fused passes: events around every 4th P/D launch pair of
+    # MID iterations, on the library's stream, over a few more epochs
+    solver.set_timing(4)
+    solver.run_epochs(max(2, min(steps, 8)))
+    solver.sync()
     kern = {}
     for kid, name in ((0, "primal_pass"), (1, "dual_pass")):
         n, tot, bpl = solver.kernel_timing(kid)
         kern[name] = {"launches_timed": n, "avg_ms": tot / max(n, 1), "bytes_per_launch": bpl}
+    solver.set_timing(0)
     info = solver.info()
     out = {
         "ms": ms_max, "iters": steps * ITERS_PER_STEP, "kernels": kern, "clocks": clk.summary(),
         "bytes_per_iteration": solver.bytes_per_iteration(), "setup_s": info.setup_time_s,
-        "norm_estimate": info.norm_estimate, "fp64_from_iteration": int(info.fp64_from_iteration),
+        "norm_estimate": info.norm_estimate, "engines": solver.engines(), "epoch_kernels": solver.epoch_kernels(),
         "scaled": solver.scaled() if precision == sp.Precision.FP64 else None,
     }
     solver.close()
     return out
 
 
+def to_tolerance(sp, torch, pinned, backend, precision, device, tol, limit_s):
+    """One sp_solve call from pinned host arrays to `tol` relative KKT (upload, scaling,
+    power iteration, iterations, solution back), timed with CUDA events on the library's
+    stream; the solution is returned for the checker, which runs outside the timing."""
+    stream = torch.cuda.ExternalStream(backend.stream(), device=f"cuda:{device}")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    params = sp.SolverParams(tolerance=tol, precision=precision, time_limit=limit_s)
+    torch.cuda.synchronize(device)
+    t0 = time.time()
+    e0.record(stream)
+    sol = sp.solve(pinned, params, backend)
+    e1.record(stream)
+    e1.synchronize()
+    return sol, e0.elapsed_time(e1) * 1e-3, time.time() - t0
+
+
+def checker_report(lp, sol, tol):
+    """The independent KKT checker (the oracle's restatement of saddlepoint-check,
+    crates/saddlepoint-check/src/lib.rs:62-118) on a GPU answer; never timed."""
+    import oracle
+
+    rep = oracle.check(lp, sol.x, sol.y)
+    return {"relative_primal": rep.relative_primal, "relative_dual": rep.relative_dual,
+            "relative_gap": rep.relative_gap, "max_relative": rep.max_relative(),
+            "passes_at": 2.0 * tol, "passed": bool(rep.max_relative() <= 2.0 * tol)}
+
+
 def run_ours(args):
-    import numpy as np
     import torch
 
     import saddlepoint_b200 as sp
@@ -260,6 +335,7 @@ def run_ours(args):
     dist = Dist(args.gpus)
     device = dist.local
     lp = powerlaw_lp(args.seed, args.scale) if args.workload == "powerlaw" else sp.generate_transport_lp(args.seed)
+    wkey = workload_key(args.workload, args.scale)
     backend = sp.CudaBackend(device)
     res = {}
     for prec in (sp.Precision.FP64, sp.Precision.Mixed):
@@ -271,17 +347,21 @@ def run_ours(args):
 
     peak, peak_kind = measured_peak()
 
-    def roofline(meas, form=""):
+    def roofline(meas, form):
         k = meas["kernels"]
         dom = max(k, key=lambda name: k[name]["avg_ms"])
         d = k[dom]
         achieved = d["bytes_per_launch"] / (d["avg_ms"] * 1e-3) / 1e9 if d["avg_ms"] > 0 else 0.0
         return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(dom + form),
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": profiled_traffic(dom, wkey, form),
+                "traffic_source": f"profiles/ncu_traffic.txt ({dom} {wkey} {form})",
                 "bytes_per_launch": d["bytes_per_launch"], "avg_launch_ms": d["avg_ms"],
                 "launches_timed": d["launches_timed"],
+                "timing": "CUDA events on the library's stream around every 4th launch of the pass, in an "
+                          "untimed pass of direct launches right after the timed graph replays",
                 "other": {name: {"achieved_gbs": k[name]["bytes_per_launch"] / (k[name]["avg_ms"] * 1e-3) / 1e9
-                                 if k[name]["avg_ms"] > 0 else None, "avg_launch_ms": k[name]["avg_ms"]}
+                                 if k[name]["avg_ms"] > 0 else None, "avg_launch_ms": k[name]["avg_ms"],
+                                 "traffic": profiled_traffic(name, wkey, form)}
                           for name in k if name != dom}}
 
     # e2e: the one-call public API from pinned host memory, K·64 iterations
@@ -301,17 +381,46 @@ def run_ours(args):
     h2d = 4 * (lp.nrows + 1) + 4 * lp.nnz + 8 * lp.nnz + 8 * (3 * lp.ncols + 2 * lp.nrows)
     d2h = 8 * (lp.ncols + lp.nrows)
     e2e = {"value": n * iters / (e2e_ms * 1e-3), "unit": "iter/s", "h2d_bytes_per_step": h2d / args.steps,
-           "d2h_bytes_per_step": d2h / args.steps, "ms_total": e2e_ms, "api": "sp_solve (one call: upload, GPU "
-           "scaling and transpose, power iteration, K*64 PDHG iterations, unscaled solution back)"}
+           "d2h_bytes_per_step": d2h / args.steps, "ms_total": e2e_ms, "iterations": iters,
+           "api": f"sp_solve (one call: upload, GPU scaling and transpose, power iteration, {iters} PDHG "
+                  "iterations, unscaled solution back)"}
+
+    # to 1e-6 relative KKT in both forms, end to end; checked outside the timing
+    tol_res = {}
+    if not args.no_tolerance:
+        golden = oracle_golden(args)
+        for prec, name in ((sp.Precision.FP64, "fp64"), (sp.Precision.Mixed, "mixed")):
+            sol_t, secs, wall = to_tolerance(sp, torch, pinned, backend, prec, device, args.tolerance,
+                                             args.tolerance_limit_s)
+            secs = dist.max(secs)
+            r = {"tolerance": args.tolerance, "status": sol_t.status.name, "iterations": int(sol_t.iterations),
+                 "restarts": int(sol_t.restarts), "seconds_e2e": secs, "wall_s": wall,
+                 "setup_s": sol_t.setup_time, "solve_s": sol_t.solve_time,
+                 "iter_per_s_solve": sol_t.iterations / sol_t.solve_time if sol_t.solve_time > 0 else None,
+                 "fp64_from_iteration": int(sol_t.fp64_from_iteration), "objective": sol_t.objective,
+                 "dual_objective": sol_t.dual_objective}
+            if dist.rank == 0:
+                r["checker"] = checker_report(lp, sol_t, args.tolerance)
+            if golden:
+                g_obj = golden["objective"]
+                r["oracle_fp64"] = {k: golden[k] for k in ("status", "iterations", "objective", "threads")}
+                r["objective_gap_vs_oracle_fp64"] = abs(sol_t.objective - g_obj) / (1.0 + abs(g_obj))
+                r["iterations_minus_oracle"] = int(sol_t.iterations) - int(golden["iterations"])
+            tol_res[name] = r
+            tol_res[name + "_obj"] = sol_t.objective
+        o64 = tol_res.pop("fp64_obj")
+        omx = tol_res.pop("mixed_obj")
+        tol_res["mixed"]["objective_gap_vs_gpu_fp64"] = abs(omx - o64) / (1.0 + abs(o64))
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(lp, f64["scaled"], f64["norm_estimate"])
 
+    batch = None
+    if args.workload == "powerlaw" and args.scale == 1.0 and not args.no_batch:
+        batch = batch_compact(sp, backend, dist, args.seed)
+
     clocks = f64["clocks"]
-    # per 64-iteration epoch: P and D of every iteration, the second (K0) P and D of the
-    # first, the Halpern x update of the first, the T pass, the controller, k_finish
-    launches_per_epoch = 2 * ITERS_PER_STEP + 6
     line = {
         "metric": "PDHG iter/s (FP64, device-resident)",
         "value": value,
@@ -325,25 +434,30 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generators of saddlepoint_b200/csrc/host.cpp)",
-        "config": dict(WORKLOAD_DESC[args.workload], parallelism=f"replicas x{n}", seed=args.seed,
-                       **({"scale": args.scale, "m": lp.nrows, "n": lp.ncols, "nnz": lp.nnz} if args.scale != 1.0 else {})),
-        "roofline": roofline(f64),
+        "config": workload_config(args),
+        "parallelism": f"replicas x{n}",
+        "roofline": roofline(f64, "fp64"),
         "e2e": e2e,
-        "gpu_launches": launches_per_epoch * args.steps,
+        "gpu_launches": f64["epoch_kernels"] * args.steps,
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "cpu_baseline": cpu,
         "forms": {
             "fp64": {"iter_per_s": value, "ms_per_step": f64["ms"] / args.steps,
                      "gb_per_iteration": f64["bytes_per_iteration"] / 1e9,
-                     "hbm_gbs_whole_iteration": f64["bytes_per_iteration"] * value / n / 1e9},
+                     "hbm_gbs_whole_iteration": f64["bytes_per_iteration"] * value / n / 1e9,
+                     "engines": {k: v for k, v in f64["engines"].items() if k.endswith("fp64")},
+                     "kernels_per_epoch": f64["epoch_kernels"],
+                     "to_tolerance": tol_res.get("fp64")},
             "mixed": {"iter_per_s": mixed_value, "ms_per_step": mix["ms"] / args.steps,
                       "gb_per_iteration": mix["bytes_per_iteration"] / 1e9,
                       "hbm_gbs_whole_iteration": mix["bytes_per_iteration"] * mixed_value / n / 1e9,
-                      "roofline": roofline(mix, "_mixed"), "clocks": mix["clocks"],
-                      "speedup_vs_fp64": mixed_value / value,
-                      "fp64_from_iteration": mix["fp64_from_iteration"],
-                      "note": "tolerances of 0: no check ends the solve or moves the SpMV to FP64 by "
-                              "accuracy; fp64_from_iteration > 0 would show the stall rule's switch"},
+                      "roofline": roofline(mix, "mixed"), "clocks": mix["clocks"],
+                      "speedup_vs_fp64": mixed_value / value, "engines": mix["engines"],
+                      "kernels_per_epoch": mix["epoch_kernels"],
+                      "to_tolerance": tol_res.get("mixed"),
+                      "note": "iter_per_s runs with tolerances of 0 (every epoch in FP32 SpMV); to_tolerance "
+                              "is the solve to 1e-6, which moves the SpMV to FP64 below 1e-5"},
+            "batch": batch,
         },
         "setup_s": f64["setup_s"],
     }
@@ -366,13 +480,15 @@ def cpu_baseline(lp, scaled, norm_estimate, iters=ITERS_PER_STEP):
 
 def run_reference(args):
     """The reference's CPU implementation of the path (the C restatement; the Rust
-    crate cannot be built here) on this arm's workload, metric and unit."""
+    crate cannot be built here) on this arm's workload, metric and unit. It generates
+    the LP with the oracle's own copy of the generators and never loads the CUDA library."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     import oracle
 
     t0 = time.time()
-    lp = powerlaw_lp(args.seed, args.scale)
+    m, n, nnz = powerlaw_shape(args.scale)
+    lp = oracle.generate_powerlaw_lp(args.seed, m, n, nnz, 1.5, 2, 5000)
     s = oracle.scaled_problem(lp)
     setup_s = time.time() - t0
     # ‖A'‖₂ only sets the step size, not the cost of an iteration: a fixed value keeps
@@ -389,13 +505,13 @@ def run_reference(args):
     value = tot_it / tot_s
     sample = (f"{args.steps} steps of {per_step} PDHG iterations ({tot_it} in one loop, a check every 64) on the C "
               f"restatement of the reference's CPU backend, {oracle.get_threads()} threads; "
-              f"generation and scaling ({setup_s:.0f} s) untimed")
+              f"generation (the oracle's copy of the generator) and scaling ({setup_s:.0f} s) untimed")
     line = {
         "impl": "reference", "metric": "PDHG iter/s (FP64, device-resident)", "value": value, "unit": "iter/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_s / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generators of saddlepoint_b200/csrc/host.cpp)",
-        "config": dict(WORKLOAD_DESC["powerlaw"], parallelism="host threads", seed=args.seed),
+        "config": workload_config(args), "parallelism": f"host threads x{oracle.get_threads()}",
         "cpu_baseline": {"value": value, "unit": "iter/s", "cores": oracle.get_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -420,26 +536,22 @@ def batch_instances(seed: int, count: int):
     return out
 
 
-def run_batch(args):
-    """Solves/s of the batched persistent kernel on the 4096-LP uneven batch (tol 1e-6),
-    against the plain device-resident form solving instances one at a time."""
+def batch_forms(sp, backend, dist, lps, runs, warm=True):
+    """Solves/s of the batched persistent kernel on `lps` in both forms (tol 1e-6): an
+    untimed first solve, then `runs` timed ones (device time of the launch, max over
+    ranks; handed-off stragglers included)."""
     import numpy as np
-    import torch
 
-    import saddlepoint_b200 as sp
-
-    dist = Dist(args.gpus)
-    count = 4096
-    lps = batch_instances(args.seed, count)
-    backend = sp.CudaBackend(dist.local)
+    count = len(lps)
     out = {}
-    for prec in (sp.Precision.FP64, sp.Precision.Mixed):
+    for prec, name in ((sp.Precision.FP64, "fp64"), (sp.Precision.Mixed, "mixed")):
         b = sp.BatchSolver(lps, sp.SolverParams(tolerance=1e-6, precision=prec), backend)
-        res, _ = b.solve()  # warm-up
+        if warm:
+            b.solve()
         times = []
         dist.barrier()
         with Clocks(dist.local) as clk:
-            for _ in range(max(1, min(args.steps, 3))):
+            for _ in range(runs):
                 res, t = b.solve()
                 times.append(t)
         t_max = dist.max(max(times))
@@ -450,21 +562,56 @@ def run_batch(args):
         # instances: 134 launches per 64-iteration epoch and about 700 for scaling,
         # transpose and power iteration each
         launches = 1 + sum(int(round(r.iterations / 64 * 134)) + 700 for r in handed)
-        out[prec] = {"solves_per_s": dist.world * count / t_max, "s_per_batch": t_max,
-                     "optimal": int((st == 0).sum()), "iterations_median": float(np.median(its)),
-                     "iterations_max": int(its.max()), "handed_off": len(handed),
-                     "handed_off_iterations": [int(r.iterations) for r in handed][:16],
+        slowest = int(np.argmax(its))
+        out[name] = {"solves_per_s": dist.world * count / t_max, "s_per_batch": t_max,
+                     "optimal": int((st == 0).sum()), "not_optimal": int((st != 0).sum()),
+                     "iterations_median": float(np.median(its)), "iterations_max": int(its.max()),
+                     "slowest_instance": slowest, "slowest_status": int(st[slowest]),
+                     "handed_off": len(handed), "handed_off_iterations": [int(r.iterations) for r in handed][:16],
+                     "variants": {"lanes": int(sum(r.variant == "lanes" for r in res)),
+                                  "tiles": int(sum(r.variant == "tiles" for r in res))},
                      "gpu_launches_per_batch": launches, "clocks": clk.summary()}
         b.close()
-    # the plain form: one device-resident solve per instance, on a spread sample
-    sample = lps[:: count // 32]
+        warm = False  # the tuner's calibration and first-launch costs are paid once per device
+    return out
+
+
+def plain_form(sp, backend, lps):
+    """The plain form on a sample of the batch: one device-resident sp_solve per instance."""
     t0 = time.time()
-    plain_ok = 0
-    for lp in sample:
+    ok = 0
+    for lp in lps:
         s = sp.solve(lp, sp.SolverParams(tolerance=1e-6), backend)
-        plain_ok += int(s.status == sp.Status.Optimal)
-    plain_s = time.time() - t0
-    plain = len(sample) / plain_s
+        ok += int(s.status == sp.Status.Optimal)
+    return {"solves_per_s": len(lps) / (time.time() - t0), "sample": len(lps), "optimal": ok}
+
+
+def batch_compact(sp, backend, dist, seed):
+    """The 4096-LP uneven batch for the default line: one untimed and one timed batch in
+    FP64, one timed batch mixed, the plain form on 32 instances, and the ratio."""
+    count = 4096
+    lps = batch_instances(seed, count)
+    forms = batch_forms(sp, backend, dist, lps, runs=1)
+    plain = plain_form(sp, backend, lps[:: count // 32])
+    return {"workload": "4096 LPs, m log-uniform [50,2000], n=2m, 3-8 nnz/col, tol 1e-6", "fp64": forms["fp64"],
+            "mixed": forms["mixed"], "plain_device_solve": plain,
+            "batched_over_plain": forms["fp64"]["solves_per_s"] / plain["solves_per_s"],
+            "mixed_batched_over_plain": forms["mixed"]["solves_per_s"] / plain["solves_per_s"]}
+
+
+def run_batch(args):
+    """Solves/s of the batched persistent kernel on the 4096-LP uneven batch (tol 1e-6),
+    against the plain device-resident form solving instances one at a time."""
+    import saddlepoint_b200 as sp
+
+    dist = Dist(args.gpus)
+    count = 4096
+    lps = batch_instances(args.seed, count)
+    backend = sp.CudaBackend(dist.local)
+    runs = max(1, min(args.steps, 3))
+    forms = batch_forms(sp, backend, dist, lps, runs)
+    sample = lps[:: count // 32]
+    plain = plain_form(sp, backend, sample)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         import oracle
@@ -477,18 +624,17 @@ def run_batch(args):
         cpu = {"value": k / (time.time() - t0), "unit": "solves/s", "cores": oracle.get_threads(), "kind": "port",
                "sample": f"{k} instances of the batch solved one after another by the C restatement (serial below "
                "32768 elements, like the reference)"}
-    f64 = out[sp.Precision.FP64]
+    f64 = forms["fp64"]
     line = {
         "metric": "batched solves/s at 1e-6 rel KKT (4096 uneven LPs)", "value": f64["solves_per_s"],
-        "unit": "solves/s", "n_gpus": dist.world, "steps": max(1, min(args.steps, 3)), "warmup": 1,
+        "unit": "solves/s", "n_gpus": dist.world, "steps": runs, "warmup": 1,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": "4096 LPs, m log-uniform [50,2000], n=2m, 3-8 nnz/col", "tolerance": 1e-6,
-                   "parallelism": f"replicas x{dist.world}"},
-        "forms": {"fp64": f64, "mixed": out[sp.Precision.Mixed],
-                  "plain_device_solve": {"solves_per_s": plain, "sample": len(sample), "optimal": plain_ok},
-                  "batched_over_plain": f64["solves_per_s"] / plain},
-        "cpu_baseline": cpu, "gpu_launches": f64["gpu_launches_per_batch"] * max(1, min(args.steps, 3)),
+        "config": {"workload": "4096 LPs, m log-uniform [50,2000], n=2m, 3-8 nnz/col", "tolerance": 1e-6},
+        "parallelism": f"replicas x{dist.world}",
+        "forms": {"fp64": f64, "mixed": forms["mixed"], "plain_device_solve": plain,
+                  "batched_over_plain": f64["solves_per_s"] / plain["solves_per_s"]},
+        "cpu_baseline": cpu, "gpu_launches": f64["gpu_launches_per_batch"] * runs,
         "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     if dist.rank == 0:
@@ -497,11 +643,26 @@ def run_batch(args):
     dist.close()
 
 
+def serve_requests(seed: int, count: int):
+    """(LP seed, m, n) of each request of the serving workload: nnz log-uniform in
+    [1e3, 1e7], n = nnz/5 columns of 5 entries, m = n/2 rows."""
+    import math
+
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nnz = math.exp(rng.uniform(math.log(1e3), math.log(1e7)))
+        n = max(10, int(nnz / 5))
+        out.append((seed * 7919 + i, max(5, n // 2), n))
+    return out
+
+
 def run_serve(args):
     """The serving loop under Poisson arrivals (λ = 200/s) of random LPs with nnz
     log-uniform in [1e3, 1e7] (n = nnz/5, m = n/2), tolerance 1e-6: p50/p99 time to
     solution and solves/s, FP64 and mixed."""
-    import math
     import threading
 
     import numpy as np
@@ -510,13 +671,9 @@ def run_serve(args):
 
     dist = Dist(args.gpus)
     nreq = max(8, min(args.steps, 400))
-    rng = np.random.default_rng(args.seed)
-    lps = []
-    for i in range(nreq):
-        nnz = math.exp(rng.uniform(math.log(1e3), math.log(1e7)))
-        n = max(10, int(nnz / 5))
-        lps.append(sp.generate_random_lp(args.seed * 7919 + i, max(5, n // 2), n, (5, 5)))
-    gaps = rng.exponential(1.0 / 200.0, size=nreq)
+    specs = serve_requests(args.seed, nreq)
+    lps = [sp.generate_random_lp(seed, m, n, (5, 5)) for seed, m, n in specs]
+    gaps = np.random.default_rng(args.seed + 1).exponential(1.0 / 200.0, size=nreq)
     backend = sp.CudaBackend(dist.local)
     forms = {}
     for prec in (sp.Precision.FP64, sp.Precision.Mixed):
@@ -536,19 +693,29 @@ def run_serve(args):
         t0 = time.time()
         with Clocks(dist.local) as clk:
             due = t0
-            for lp, g in zip(lps, gaps):
+            index = {}
+            for i, (lp, g) in enumerate(zip(lps, gaps)):
                 due += g
                 delay = due - time.time()
                 if delay > 0:
                     time.sleep(delay)
-                srv.submit(lp)
+                index[srv.submit(lp)] = i
             th.join()
         wall = time.time() - t0
         srv.close()
-        lat = np.array([r.total_s for r in results])
-        forms[prec] = {"solves_per_s": nreq / wall, "p50_s": float(np.percentile(lat, 50)),
-                       "p99_s": float(np.percentile(lat, 99)),
-                       "optimal": int(sum(r.status == 0 for r in results)), "requests": nreq,
+        ok = [r for r in results if r.status == 0]
+        lat = np.array([r.total_s for r in ok]) if ok else np.array([float("nan")])
+        lat_all = np.array([r.total_s for r in results])
+        forms[prec] = {"solves_per_s": len(ok) / wall, "requests_per_s": nreq / wall,
+                       "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                       "latency_over": "requests that reached Optimal (time to 1e-6)",
+                       "optimal": len(ok), "not_optimal": nreq - len(ok), "requests": nreq,
+                       "not_optimal_requests": sorted(
+                           ({"index": index[r.id], "lp_seed": specs[index[r.id]][0], "nrows": specs[index[r.id]][1],
+                             "ncols": specs[index[r.id]][2], "status": int(r.status), "iterations": int(r.iterations),
+                             "rel_primal": r.primal_residual, "rel_dual": r.dual_residual}
+                            for r in results if r.status != 0), key=lambda d: d["index"]),
+                       "p50_all_s": float(np.percentile(lat_all, 50)),
                        "queue_p50_s": float(np.median([r.queue_s for r in results])), "clocks": clk.summary()}
     f64 = forms[sp.Precision.FP64]
     line = {
@@ -556,7 +723,9 @@ def run_serve(args):
         "unit": "solves/s", "n_gpus": dist.world, "steps": nreq, "warmup": 0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
         "config": {"workload": "Poisson arrivals 200/s, nnz log-uniform [1e3,1e7], n=nnz/5, m=n/2",
-                   "budget_bytes": 150e9, "max_inflight": 8, "batch_max_nnz": 50_000, "requests": nreq},
+                   "budget_bytes": 150e9, "max_inflight": 8, "batch_max_nnz": 50_000, "requests": nreq,
+                   "max_iterations": 200_000},
+        "parallelism": f"replicas x{dist.world}",
         "forms": {"fp64": f64, "mixed": forms[sp.Precision.Mixed]},
         "p50_s": f64["p50_s"], "p99_s": f64["p99_s"],
         "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},

@@ -4,8 +4,8 @@
  *
  * Part 1 mirrors the reference's fused `Backend` trait
  * (crates/saddlepoint-core/src/backend.rs:43-137) one entry point per method,
- * so that a Rust shim crate can implement `Backend` by calling these functions
- * (see INTEGRATION.md). Vectors and problems are opaque handles owned by the
+ * so that a Rust shim crate can implement `Backend` by calling these functions.
+ * Vectors and problems are opaque handles owned by the
  * library; reductions return their scalars through out-pointers, exactly like
  * the trait returns host `f64`s and stats structs.
  *
@@ -226,6 +226,14 @@ int sp_solver_set_timing(sp_solver *s, int every);
 int sp_solver_kernel_timing(sp_solver *s, int id, int64_t *launches, double *total_ms, double *bytes_per_launch);
 /* Algorithmic bytes of one PDHG iteration in the current precision. */
 double sp_solver_bytes_per_iteration(sp_solver *s);
+/* Which engine runs each fused pass of the solver (chosen at creation from the
+ * problem's size, or SP_PASS_ENGINE): out[0] primal FP64, out[1] primal FP32,
+ * out[2] dual FP64, out[3] dual FP32 (the FP32 entries apply to the mixed form). */
+enum { SP_ENGINE_TILES = 0, SP_ENGINE_STREAM = 1, SP_ENGINE_SELL = 2 };
+int sp_solver_engines(sp_solver *s, int32_t out[4]);
+/* Kernel launches of one epoch of check_every iterations, counted from the
+ * kernel nodes of its CUDA graph (the graph is built if it does not exist yet). */
+int sp_solver_epoch_kernels(sp_solver *s, int64_t *count);
 /* Downloads the scaled problem the solver built on the device (ScaledProblem,
  * scaling.rs:36-50): A' and A'ᵀ in CSR, c', lc', uc', lv', uv', the row and
  * column scales and the two scalar rescalings. Any pointer may be null. */
@@ -285,7 +293,10 @@ int sp_server_create(sp_ctx *ctx, const sp_server_config *cfg, const sp_solver_p
 /* Copies the LP; returns at once with a request id. */
 int sp_server_submit(sp_server *s, const sp_lp *lp, int64_t *id);
 /* Waits for the next finished request (timeout_s < 0: wait forever). Returns
- * SP_OK with *got = 1 when a result was written, *got = 0 on timeout. */
+ * SP_OK with *got = 1 when a result was written, *got = 0 on timeout. x and y may
+ * be null (no solution copied); a non-null x or y with room for fewer than the
+ * request's n or m values returns SP_ERR_INVALID with *got = 0 and leaves the
+ * result queued for the next poll. */
 int sp_server_poll(sp_server *s, double timeout_s, sp_server_result *out, double *x, int64_t xcap, double *y,
                    int64_t ycap, int *got);
 /* Footprint the admission control charges for an LP of this shape. */

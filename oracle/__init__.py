@@ -117,6 +117,14 @@ class RayStats(C.Structure):
     _fields_ = [("objective", dbl), ("violation_sq", dbl), ("norm_sq", dbl)]
 
 
+class GenParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("seed", u64), ("nrows", i64), ("ncols", i64), ("nnz_per_col_min", i64),
+        ("nnz_per_col_max", i64), ("target_nnz", i64), ("zipf_s", dbl), ("degree_min", i64), ("degree_max", i64),
+        ("supplies", i64), ("demands", i64),
+    ]
+
+
 class Pid(C.Structure):
     _fields_ = [("integral", dbl), ("prev_error", dbl), ("has_prev", C.c_int), ("best_weight", dbl), ("best_balance", dbl)]
 
@@ -135,7 +143,7 @@ def build(force: bool = False) -> str:
 
 def _stale() -> bool:
     t = os.path.getmtime(_LIB_PATH)
-    return any(os.path.getmtime(os.path.join(_HERE, f)) > t for f in ("sp_oracle.c", "sp_mps.c", "sp_oracle.h"))
+    return any(os.path.getmtime(os.path.join(_HERE, f)) > t for f in ("sp_oracle.c", "sp_mps.c", "sp_gen.c", "sp_oracle.h"))
 
 
 def lib():
@@ -186,6 +194,7 @@ def lib():
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         L.or_lp_validate.argtypes = [C.POINTER(Lp)]
+        L.or_generate.argtypes = [C.POINTER(GenParams), C.POINTER(Lp)]
     return _lib
 
 
@@ -281,6 +290,46 @@ def read_mps(text: bytes, name: str = "") -> OracleLp:
     )
     L.or_lp_free(C.byref(lp))
     return out
+
+
+def _take(lp: Lp, name: str) -> OracleLp:
+    m, n = lp.a.nrows, lp.a.ncols
+    rp, ci, v = _csr_to_np(lp.a)
+    out = OracleLp(
+        nrows=m, ncols=n, row_ptr=rp, col_idx=ci, values=v, c=_arr(lp.c, n), lc=_arr(lp.lc, m),
+        uc=_arr(lp.uc, m), lv=_arr(lp.lv, n), uv=_arr(lp.uv, n), c0=lp.c0, maximize=bool(lp.maximize), name=name,
+    )
+    lib().or_lp_free(C.byref(lp))
+    return out
+
+
+def _generate(g: GenParams, name: str) -> OracleLp:
+    lp = Lp()
+    rc = lib().or_generate(C.byref(g), C.byref(lp))
+    if rc != 0:
+        raise ValueError(f"generator rejected its parameters ({rc})")
+    return _take(lp, name)
+
+
+def generate_random_lp(seed: int, nrows: int, ncols: int, nnz_per_col=(5, 5)) -> OracleLp:
+    """The random LP recipe (the CUDA library's generate_random_lp, the same arrays)."""
+    g = GenParams(kind=0, seed=seed, nrows=nrows, ncols=ncols, nnz_per_col_min=nnz_per_col[0],
+                  nnz_per_col_max=nnz_per_col[1])
+    return _generate(g, f"random_{nrows}x{ncols}_s{seed}")
+
+
+def generate_powerlaw_lp(seed: int, nrows: int, ncols: int, target_nnz: int, zipf_s: float = 1.5,
+                         degree_min: int = 2, degree_max: int = 5000) -> OracleLp:
+    """Power-law column degrees (the CUDA library's generate_powerlaw_lp, the same arrays)."""
+    g = GenParams(kind=1, seed=seed, nrows=nrows, ncols=ncols, target_nnz=target_nnz, zipf_s=zipf_s,
+                  degree_min=degree_min, degree_max=degree_max)
+    return _generate(g, f"powerlaw_{nrows}x{ncols}_{target_nnz}_s{seed}")
+
+
+def generate_transport_lp(seed: int, supplies: int = 2000, demands: int = 2000) -> OracleLp:
+    """Transportation LP (the CUDA library's generate_transport_lp, the same arrays)."""
+    g = GenParams(kind=2, seed=seed, supplies=supplies, demands=demands)
+    return _generate(g, f"transport_{supplies}x{demands}_s{seed}")
 
 
 def from_triplets(nrows: int, ncols: int, rows, cols, vals):

@@ -183,6 +183,22 @@ double or_pid_update(or_pid *pid, const or_solver_params *p, double omega, doubl
 void or_check(const or_lp *p, const double *x, const double *y, or_kkt_report *out);
 double or_kkt_max_relative(const or_kkt_report *r);
 
+/* ---- seeded synthetic generators (sp_gen.c) --------------------------------- */
+/* kind 0: random LP (nnz_per_col_min..max per column), 1: power-law columns
+ * (Zipf(zipf_s) on [degree_min, degree_max] rescaled to target_nnz), 2: transportation
+ * LP (supplies x demands). The same draws as the CUDA library's sp_generate. */
+typedef struct {
+    int kind;
+    uint64_t seed;
+    int64_t nrows, ncols;
+    int64_t nnz_per_col_min, nnz_per_col_max;
+    int64_t target_nnz;
+    double zipf_s;
+    int64_t degree_min, degree_max;
+    int64_t supplies, demands;
+} or_gen_params;
+int or_generate(const or_gen_params *g, or_lp *out);
+
 /* ---- MPS reader (crates/saddlepoint-io/src/lib.rs:59-309) -------------------- */
 /* Returns OR_OK or OR_ERR_PARSE with *err_line set (1-based) and err text. */
 int or_read_mps(const char *text, size_t len, or_lp *out, int64_t *err_line, char *err, size_t errlen);

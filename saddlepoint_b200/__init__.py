@@ -505,6 +505,22 @@ class Solver(_Handle):
     def bytes_per_iteration(self) -> float:
         return float(self.lib.sp_solver_bytes_per_iteration(self.h))
 
+    ENGINES = {0: "tiles", 1: "stream", 2: "sell"}
+
+    def engines(self) -> dict:
+        """The engine of each fused pass: {'primal_fp64', 'primal_fp32', 'dual_fp64', 'dual_fp32'}
+        -> 'tiles' | 'stream' | 'sell' (the FP32 entries apply to the mixed form)."""
+        out = (C.c_int32 * 4)()
+        self._c(self.lib.sp_solver_engines(self.h, out))
+        keys = ("primal_fp64", "primal_fp32", "dual_fp64", "dual_fp32")
+        return {k: self.ENGINES[int(v)] for k, v in zip(keys, out)}
+
+    def epoch_kernels(self) -> int:
+        """Kernel launches in one epoch of check_every iterations (its graph's kernel nodes)."""
+        n = C.c_int64()
+        self._c(self.lib.sp_solver_epoch_kernels(self.h, C.byref(n)))
+        return int(n.value)
+
     def scaled(self) -> ScaledProblem:
         p = self.problem
         m, n, nnz = p.nrows, p.ncols, p.nnz

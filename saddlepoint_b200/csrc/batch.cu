@@ -108,9 +108,9 @@ int calibrate(sp_ctx *ctx, TuneTable *T) {
         A2.base.tolerance = 0.0;  // never converged: every run takes exactly its iterations
         A2.handoff_ns = 0;
         A2.power_iterations = std::min<unsigned long long>(A2.power_iterations, 4);
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
+        EventPair ep;
+        if (!rc) rc = ep.init();
+        cudaEvent_t e0 = ep.e0, e1 = ep.e1;
         auto run = [&](int c, unsigned long long iters, float *ms_out) -> int {
             const BatchInst &I = inst[c];
             A2.base.max_iterations = iters;
@@ -140,8 +140,6 @@ int calibrate(sp_ctx *ctx, TuneTable *T) {
                 T->nnz[p] = inst[p].nnz;
             }
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         T->npts = npts;
         T->ready = rc == SP_OK;
     }
@@ -600,17 +598,14 @@ extern "C" int sp_batch_solve(sp_batch *b, sp_batch_result *results, double *ela
     int rc = enter(b->ctx);
     if (rc) return rc;
     cudaStream_t st = b->ctx->stream;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
+    EventPair ep;
+    if ((rc = ep.init())) return rc;
+    SP_CUDA_TRY(cudaEventRecord(ep.e0, st));
     SP_CUDA_TRY(cudaGraphLaunch(b->graph, st));
-    cudaEventRecord(e1, st);
-    SP_CUDA_TRY(cudaEventSynchronize(e1));
+    SP_CUDA_TRY(cudaEventRecord(ep.e1, st));
+    SP_CUDA_TRY(cudaEventSynchronize(ep.e1));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    SP_CUDA_TRY(cudaEventElapsedTime(&ms, ep.e0, ep.e1));
     std::vector<sp_batch_result> res(b->count);
     SP_CUDA_TRY(cudaMemcpy(res.data(), b->args.res, sizeof(sp_batch_result) * b->count, cudaMemcpyDeviceToHost));
     const auto t0 = std::chrono::steady_clock::now();

@@ -155,4 +155,18 @@ struct Err {
 int fail(int code, const std::string &msg);  // records the error on the current thread's context
 void set_current_ctx(sp_ctx *ctx);
 
+// Two timing events, created by init() (checked) and destroyed with the object.
+struct EventPair {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int init() {
+        SP_CUDA_TRY(cudaEventCreate(&e0));
+        SP_CUDA_TRY(cudaEventCreate(&e1));
+        return SP_OK;
+    }
+    ~EventPair() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
 }  // namespace sp

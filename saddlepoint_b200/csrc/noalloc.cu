@@ -79,12 +79,16 @@ int scratch_for_current_device(double **out) {
 extern "C" int sp_dot_noalloc(const double *a, const double *b, int64_t n, double *result, void *stream) {
     if (n < 0 || !result || (n > 0 && (!a || !b))) return SP_ERR_INVALID;
     if (n > SP_NOALLOC_DOT_MAX_N) return SP_ERR_TOO_LARGE;
+    // an error already pending on this thread belongs to the caller's earlier work:
+    // report it without consuming it, and launch nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return SP_ERR_CUDA;
     double *partials = nullptr;
     int rc = scratch_for_current_device(&partials);
     if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = n > 0 ? (int)((n + kPerBlock - 1) / kPerBlock) : 1;
     k_dot_partials<<<blocks, kThreads, 0, s>>>(a, b, n, partials);
+    if (cudaGetLastError() != cudaSuccess) return SP_ERR_CUDA;
     k_dot_finish<<<1, kThreads, 0, s>>>(partials, blocks, result);
     return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
 }

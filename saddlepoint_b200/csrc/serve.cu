@@ -265,11 +265,14 @@ extern "C" int sp_server_poll(sp_server *s, double timeout_s, sp_server_result *
         else s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready);
         if (s->finished.empty()) return SP_OK;
         r = s->finished.front();
+        // a solution buffer too small for this result: leave the result queued so the
+        // caller can poll again with larger buffers
+        if ((x && xcap < (int64_t)r->x.size()) || (y && ycap < (int64_t)r->y.size())) return SP_ERR_INVALID;
         s->finished.pop_front();
     }
     *out = r->res;
-    if (x && xcap >= (int64_t)r->x.size()) memcpy(x, r->x.data(), sizeof(double) * r->x.size());
-    if (y && ycap >= (int64_t)r->y.size()) memcpy(y, r->y.data(), sizeof(double) * r->y.size());
+    if (x) memcpy(x, r->x.data(), sizeof(double) * r->x.size());
+    if (y) memcpy(y, r->y.data(), sizeof(double) * r->y.size());
     int err = r->error;
     delete r;
     *got = 1;

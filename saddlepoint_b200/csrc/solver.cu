@@ -515,16 +515,18 @@ struct StreamKernel {
         return SP_OK;
     }
     template <int GW, bool LDG, int B, bool DEEP>
-    static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op) {
-        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op);
+    static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op, const StreamTrial &tr) {
+        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op, tr);
     }
-    static void launch(const sp_ctx *ctx, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ctx->sms, M.ntiles));
+    static void launch(const sp_solver *s, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(s->ctx->sms, M.ntiles));
+        StreamTrial tr = s->trial;
+        if (tr.withhold >= 0) tr.withhold += M.nlong;  // the knob counts the tiles after the long rows
         switch (variant) {
-        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op); break;
-        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op); break;
-        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op); break;
-        default: go<4, false, 1, false>(grid, M, st, op); break;
+        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op, tr); break;
+        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op, tr); break;
+        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op, tr); break;
+        default: go<4, false, 1, false>(grid, M, st, op, tr); break;
         }
     }
 };
@@ -712,17 +714,24 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
 // A problem under SMALL_NNZ nonzeros keeps both passes on the tile engine: there an
 // iteration's time is launch latency and tile parallelism (32 LPs of the batch workload,
 // one device solve each: 9.1 µs per iteration on tiles, 9.5 stream, 11.6 SELL).
-// SP_PASS_ENGINE=tiles|stream|sell overrides all four; SP_STREAM_GATHER names the
-// stream variant.
+// SP_PASS_ENGINE=tiles|stream|sell overrides all four (large: the assignment above for a
+// problem of any size); SP_STREAM_GATHER names the stream variant.
 constexpr int64_t SMALL_NNZ = 1 << 20;
 
 int choose_engines(sp_solver *s) {
-    const bool small = s->nnz < SMALL_NNZ;
+    const char *eng = getenv("SP_PASS_ENGINE");
+    // "large": the large-problem assignment whatever the size (tests of small LPs use it)
+    const bool small = s->nnz < SMALL_NNZ && !(eng && !strcmp(eng, "large"));
     s->sv_p64 = small ? -1 : SV_LDG4_DEEP;
     s->sv_p32 = small ? -1 : SV_LDG4;
     s->sv_d64 = small ? -1 : ENGINE_SELL;
     s->sv_d32 = small ? -1 : ENGINE_SELL;
-    const char *eng = getenv("SP_PASS_ENGINE");
+    // test knob of the stream engine's stall path (stream.cuh: StreamTrial): the copies
+    // of one tile are never issued and every wait gives up after 100 µs
+    if (const char *w = getenv("SP_TEST_STREAM_WITHHOLD")) {
+        s->trial.withhold = std::max(0, atoi(w));
+        s->trial.wait_ns = 100000ull;
+    }
     if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
     if (eng && !strcmp(eng, "sell")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = ENGINE_SELL;
     if (eng && !strcmp(eng, "stream")) {
@@ -774,11 +783,11 @@ void launch_P(sp_solver *s, int i, int role, cudaStream_t st) {
     if ((role == ROLE_MID || role == ROLE_FIRST) && (s->sv_p64 >= 0 || (s->mixed && s->sv_p32 >= 0))) {
         if (s->mixed) {
             if (s->sv_p32 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<true, 0>(p, i, role));
-            else if (s->sv_p32 >= 0) StreamP32::launch(s->ctx, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
+            else if (s->sv_p32 >= 0) StreamP32::launch(s, s->AT, st, mkP<true, 0>(p, i, role), s->sv_p32);
             else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 0>(p, i, role));
         }
         if (s->sv_p64 == ENGINE_SELL) launch_sell(s, s->sellAT, st, mkP<false, 0>(p, i, role));
-        else if (s->sv_p64 >= 0) StreamP64::launch(s->ctx, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
+        else if (s->sv_p64 >= 0) StreamP64::launch(s, s->AT, st, mkP<false, 0>(p, i, role), s->sv_p64);
         else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<false, 0>(p, i, role));
         if (role == ROLE_FIRST) {
             if (s->mixed) launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, sm, st, mkP<true, 1>(p, i, role), mkP<false, 1>(p, i, role));
@@ -821,11 +830,11 @@ void launch_D(sp_solver *s, int i, int role, cudaStream_t st) {
         const size_t s1 = tile_smem_bytes<1, double>();
         if (s->mixed) {
             if (s->sv_d32 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<true, 0>(p, i, role));
-            else if (s->sv_d32 >= 0) StreamD32::launch(s->ctx, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
+            else if (s->sv_d32 >= 0) StreamD32::launch(s, s->A, st, mkD<true, 0>(p, i, role), s->sv_d32);
             else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, s1, st, mkD<true, 0>(p, i, role));
         }
         if (s->sv_d64 == ENGINE_SELL) launch_sell(s, s->sellA, st, mkD<false, 0>(p, i, role));
-        else if (s->sv_d64 >= 0) StreamD64::launch(s->ctx, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
+        else if (s->sv_d64 >= 0) StreamD64::launch(s, s->A, st, mkD<false, 0>(p, i, role), s->sv_d64);
         else launch_tiles(s->ctx->sms, s->ctx->d_tiles, g, s1, st, mkD<false, 0>(p, i, role));
         if (role == ROLE_FIRST) {
             // the k = 0 variant: two products and two partial sums per row
@@ -883,14 +892,15 @@ void enqueue_epoch(sp_solver *s, int E, cudaStream_t st, bool timed) {
     for (int i = 0; i < E; ++i) {
         const bool last = i == E - 1;
         const int role = last ? ROLE_CHECK : (i == 0 ? ROLE_FIRST : ROLE_MID);
-        const bool sample = timed && role == ROLE_MID && s->timing_every > 0 && (s->timing_counter++ % s->timing_every == 0);
+        bool sample = timed && role == ROLE_MID && s->timing_every > 0 && (s->timing_counter++ % s->timing_every == 0);
         cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
         if (sample) {
             e0 = s->event();
             e1 = s->event();
             e2 = s->event();
-            cudaEventRecord(e0, st);
+            sample = e0 && e1 && e2;  // no sample where the pool could not grow
         }
+        if (sample) cudaEventRecord(e0, st);
         launch_P(s, i, role, st);
         if (sample) cudaEventRecord(e1, st);
         launch_D(s, i, role, st);
@@ -930,6 +940,18 @@ int build_graph(sp_solver *s, int E, cudaGraphExec_t *out) {
     SP_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     enqueue_epoch(s, E, st, false);
     SP_CUDA_TRY(cudaStreamEndCapture(st, &g));
+    // the epoch's kernel launches, for the callers that count them
+    size_t nodes = 0;
+    int64_t kernels = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+        std::vector<cudaGraphNode_t> all(nodes);
+        if (cudaGraphGetNodes(g, all.data(), &nodes) == cudaSuccess)
+            for (size_t k = 0; k < nodes; ++k) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(all[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+            }
+    }
+    s->graph_kernels[E] = kernels;
     cudaError_t e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(SP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
@@ -1397,8 +1419,19 @@ extern "C" int sp_solver_solve(sp_solver *s, sp_solution_info *info) {
     const double limit = s->prm.time_limit_s;
     // Epochs are queued SolverLookahead ahead of the state the host has seen;
     // each queued epoch is followed by a copy of the state into its own slot.
-    std::vector<cudaEvent_t> ev(SolverLookahead + 1);
-    for (auto &e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    // the epochs' completion events, destroyed on every way out
+    struct Events {
+        std::vector<cudaEvent_t> e;
+        ~Events() {
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } events;
+    for (int k = 0; k < SolverLookahead + 1; ++k) {
+        cudaEvent_t e = nullptr;
+        SP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        events.e.push_back(e);
+    }
+    std::vector<cudaEvent_t> &ev = events.e;
     uint64_t queued = 0, seen = 0;
     bool stop = false;
     DevState last{};
@@ -1436,13 +1469,12 @@ extern "C" int sp_solver_solve(sp_solver *s, sp_solution_info *info) {
         }
     }
     SP_CUDA_TRY(cudaStreamSynchronize(st));
-    for (auto &e : ev) cudaEventDestroy(e);
     SP_CUDA_TRY(cudaMemcpy(s->h_st, s->d_st, sizeof(DevState), cudaMemcpyDeviceToHost));
     last = s->h_st[0];
     s->solve_s = now_s() - t0;
     if (last.error == ERR_NUMERICAL_ITERATES) return fail(SP_ERR_NUMERICAL, "numerical breakdown: iterates are not finite");
     if (last.error == ERR_PIPELINE_STALL)
-        return fail(SP_ERR_CUDA, "a bulk copy of the pass pipeline did not complete within one second");
+        return fail(SP_ERR_CUDA, "a bulk copy of the pass pipeline did not complete within its wait limit");
     if (!last.done && !s->time_limited) s->time_limited = true;  // only reachable with an exhausted limit
     fill_info(s, last, info);
     return SP_OK;
@@ -1521,6 +1553,24 @@ extern "C" int sp_solver_kernel_timing(sp_solver *s, int id, int64_t *launches, 
 }
 
 extern "C" double sp_solver_bytes_per_iteration(sp_solver *s) { return s ? s->pass_bytes(0) + s->pass_bytes(1) : 0.0; }
+
+extern "C" int sp_solver_engines(sp_solver *s, int32_t out[4]) {
+    if (!s || !out) return SP_ERR_INVALID;
+    const int v[4] = {s->sv_p64, s->sv_p32, s->sv_d64, s->sv_d32};
+    for (int k = 0; k < 4; ++k) out[k] = v[k] < 0 ? SP_ENGINE_TILES : (v[k] == ENGINE_SELL ? SP_ENGINE_SELL : SP_ENGINE_STREAM);
+    return SP_OK;
+}
+
+extern "C" int sp_solver_epoch_kernels(sp_solver *s, int64_t *count) {
+    if (!s || !count) return SP_ERR_INVALID;
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    const int E = (int)std::max<uint64_t>(1, s->prm.check_every);
+    cudaGraphExec_t g;
+    if ((rc = epoch_graph(s, E, &g))) return rc;
+    *count = s->graph_kernels[E];
+    return SP_OK;
+}
 
 extern "C" void sp_solver_free(sp_solver *s) { solver_release(s); }
 

@@ -6,6 +6,7 @@
 
 #include "internal.cuh"
 #include "sell.cuh"
+#include "stream.cuh"
 
 namespace sp {
 constexpr int SolverLookahead = 2;  // epochs queued ahead of the state the host has read
@@ -21,6 +22,7 @@ struct sp_solver {
     // engine of each MID pass: -1 the tile engine, ENGINE_SELL the SELL path (sell.cuh),
     // else a stream-engine variant (stream.cuh)
     int sv_p64 = -1, sv_p32 = -1, sv_d64 = -1, sv_d32 = -1;
+    sp::StreamTrial trial;      // wait limits of the stream engine (and its test knob)
     sp::SellMat sellA, sellAT;  // SELL copies of A' (dual pass) and A'ᵀ (primal pass), when used
     cudaStream_t aux = nullptr;  // second stream of a SELL pass: its warp rows beside its windows
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -54,6 +56,7 @@ struct sp_solver {
     sp_check_record *d_trace = nullptr;
     int64_t trace_cap = 0;
     std::map<int, cudaGraphExec_t> graphs;  // epoch length -> instantiated graph
+    std::map<int, int64_t> graph_kernels;    // epoch length -> kernel nodes of its graph
     uint64_t launched = 0;
     bool time_limited = false;
     double setup_s = 0, solve_s = 0;
@@ -65,10 +68,14 @@ struct sp_solver {
     std::vector<cudaEvent_t> event_pool;
     size_t event_next = 0;
 
+    // A timing event from the pool (null when none can be created).
     cudaEvent_t event() {
         if (event_next == event_pool.size()) {
-            cudaEvent_t e;
-            cudaEventCreate(&e);
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
             event_pool.push_back(e);
         }
         return event_pool[event_next++];

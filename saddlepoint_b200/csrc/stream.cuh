@@ -65,6 +65,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 constexpr unsigned long long STREAM_WAIT_NS = 1000000000ull;
 
+// Limits of a launch's waits. `withhold` >= 0 is a test knob (set only from the
+// SP_TEST_STREAM_WITHHOLD environment variable when a solver is created): the loader
+// never issues the copies of that tile, so the roles waiting for it run out of their
+// `wait_ns` and take the stall path, with no copy in flight and nothing faulted.
+struct StreamTrial {
+    unsigned long long wait_ns = STREAM_WAIT_NS;
+    int withhold = -1;
+};
+
 // Waits for the phase of parity `parity` to complete; false after one second.
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -75,12 +84,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 }
 
 // Bounded wait that also gives up once another role has raised the abort flag.
-__device__ __forceinline__ bool stream_wait(unsigned long long *bar, unsigned parity, volatile int *abort) {
+__device__ __forceinline__ bool stream_wait(unsigned long long *bar, unsigned parity, volatile int *abort,
+                                            unsigned long long limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort) return false;
-        if (global_ns() - t0 > STREAM_WAIT_NS) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
     return true;
 }
@@ -230,7 +240,7 @@ __device__ __forceinline__ void consumer_long_row(Op &op, double *sh, int tile) 
 // then the products stored over the values and a plain arrive) instead of cp.async;
 // DEEP: the slot count (StreamLayout).
 template <int GW, bool LDG, int B, bool DEEP, class Op>
-__device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntiles, int nlong) {
+__device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntiles, int nlong, const StreamTrial tr) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
     using ST = typename Op::ST;
@@ -265,10 +275,11 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
         unsigned pend = 0, par = 0;  // slots with a copy outstanding and its phase parity
         for (int j = 0; j < nmine; ++j) {
             const int s = j % S, k = j / S;
-            if (k >= 1 && !stream_wait(bar_empty + s, (unsigned)(k - 1) & 1u, abort_v)) {
+            if (k >= 1 && !stream_wait(bar_empty + s, (unsigned)(k - 1) & 1u, abort_v, tr.wait_ns)) {
                 stream_abort(op, abort);
                 break;
             }
+            if (first + j * step == tr.withhold) continue;  // test knob: no copy, no arrival
             const Tile t = op.tiles[first + j * step];
             const int ka = t.z & ~(L::IA - 1), kb = (t.w + L::IA - 1) & ~(L::IA - 1);
             const int va = t.z & ~(L::VA - 1), vb = (t.w + L::VA - 1) & ~(L::VA - 1);
@@ -302,7 +313,7 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
         const GT *__restrict__ gv = op.gvec();
         for (int j = 0; j < nmine; ++j) {
             const int s = j % S, k = j / S;
-            if (!stream_wait(bar_load + s, (unsigned)k & 1u, abort_v)) {
+            if (!stream_wait(bar_load + s, (unsigned)k & 1u, abort_v, tr.wait_ns)) {
                 stream_abort(op, abort);
                 break;
             }
@@ -346,8 +357,8 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
     double part[1] = {0.0};
     for (int j = 0; j < nmine; ++j) {
         const int s = j % S, k = j / S;
-        if (!stream_wait(bar_load + s, (unsigned)k & 1u, abort_v) ||
-            !stream_wait(bar_gath + s, (unsigned)k & 1u, abort_v)) {
+        if (!stream_wait(bar_load + s, (unsigned)k & 1u, abort_v, tr.wait_ns) ||
+            !stream_wait(bar_gath + s, (unsigned)k & 1u, abort_v, tr.wait_ns)) {
             stream_abort(op, abort);
             break;
         }
@@ -406,9 +417,9 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
 // depends only on the device state). One CTA of stream_threads(GW) per SM, with
 // StreamLayout<Op, !LDG, DEEP>::total bytes of dynamic shared memory.
 template <class Op, int GW, bool LDG, int B, bool DEEP>
-__global__ void __launch_bounds__(stream_threads(GW), 1) k_stream(int ntiles, int nlong, Op op) {
+__global__ void __launch_bounds__(stream_threads(GW), 1) k_stream(int ntiles, int nlong, Op op, StreamTrial tr) {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (op.setup()) stream_run<GW, LDG, B, DEEP>(op, smem, ntiles, nlong);
+    if (op.setup()) stream_run<GW, LDG, B, DEEP>(op, smem, ntiles, nlong, tr);
 }
 
 }  // namespace sp

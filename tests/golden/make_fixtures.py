@@ -2,7 +2,7 @@
 
 Run in the build container (the reference tree is not present on GPU machines):
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <reference tree>
 
 It copies the reference's own test data for this path, unchanged in content:
   * data/netlib/*.mps  -> tests/golden/netlib/<name>.mps.gz  (gzip of the file bytes)
@@ -36,4 +36,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <path of the reference source tree>")
+    main(sys.argv[1])

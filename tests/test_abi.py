@@ -106,3 +106,23 @@ def test_server_footprint_grows_with_size():
     f2 = sp.Server.footprint(100_000, 200_000, 1_000_000)
     assert 0 < f1 < f2
     assert sp.Server.footprint(10, 20, 100, 1) > sp.Server.footprint(10, 20, 100, 0)
+
+
+@pytest.mark.parametrize("kind,args", [
+    ("random", (3, 50, 100, (3, 8))), ("random", (11, 500, 1000, (5, 5))), ("random", (7, 2000, 4000, (1, 40))),
+    ("powerlaw", (5, 2000, 4000, 40_000)), ("powerlaw", (3, 20_000, 40_000, 400_000)),
+    ("powerlaw", (1, 200, 400, 20_000)), ("transport", (1, 30, 40)), ("transport", (5, 300, 300)),
+])
+def test_generators_equal_the_oracle_copy(kind, args):
+    """The library's seeded generators (host code) and the oracle's C copy build the same
+    arrays bit for bit; the oracle's copy is what the CPU-side benchmark arm and the
+    fixture script use, so they never load the library."""
+    import oracle
+
+    ours = getattr(sp, f"generate_{kind}_lp")(*args)
+    ref = getattr(oracle, f"generate_{kind}_lp")(*args)
+    assert (ours.nrows, ours.ncols, ours.nnz) == (ref.nrows, ref.ncols, ref.nnz)
+    assert np.array_equal(ours.row_ptr, ref.row_ptr)
+    assert np.array_equal(ours.col_idx.astype(np.int64), ref.col_idx)
+    for k in ("values", "c", "lc", "uc", "lv", "uv"):
+        assert np.array_equal(getattr(ours, k), getattr(ref, k)), k

@@ -190,3 +190,38 @@ def test_netlib_read_by_the_library_solves_like_the_oracle(name, gpu_backend):
     lp = sp().read_mps(f"{NETLIB}/{name}.mps.gz")
     g = sp().solve(lp, sp().SolverParams(tolerance=TOL), gpu_backend)
     compare(name, netlib_lp(name), g, reference_solution(name))
+
+
+@pytest.mark.parametrize("name", ["afiro", "israel", "shell", "25fv47", "80bau3b"])
+def test_norm_estimate_matches_oracle(name, gpu_backend):
+    """Solver::estimate_norm (solver.rs:215-242): the device power iteration gives the
+    oracle's ‖A'‖₂ estimate to 1e-12 relative."""
+    lp = netlib_lp(name)
+    s = oracle.scaled_problem(lp)
+    ref = oracle.solve_scaled(lp, s, tolerance=TOL, stop_after=1)
+    g = sp().Solver(lp, sp().SolverParams(tolerance=TOL), gpu_backend).info()
+    assert math.isclose(g.norm_estimate, ref.norm_estimate, rel_tol=1e-12), (g.norm_estimate, ref.norm_estimate)
+
+
+def test_norm_estimate_matches_oracle_on_powerlaw_lp(gpu_backend):
+    lp = sp().generate_powerlaw_lp(5, 20_000, 40_000, 400_000)
+    s = oracle.scaled_problem(lp)
+    ref = oracle.solve_scaled(lp, s, tolerance=TOL, stop_after=1)
+    g = sp().Solver(lp, sp().SolverParams(tolerance=TOL), gpu_backend).info()
+    assert math.isclose(g.norm_estimate, ref.norm_estimate, rel_tol=1e-12), (g.norm_estimate, ref.norm_estimate)
+
+
+def test_collapsed_power_iteration_is_a_numerical_error(gpu_backend):
+    """A'v = 0 for the power iteration's start vector (one row, +1 and -1 on columns 0 and
+    7, whose start entries are equal): the reference returns SolveError::Numerical
+    ("power iteration collapsed", solver.rs:229-231); so do the oracle and the GPU."""
+    inf = math.inf
+    rp, ci, v = oracle.from_triplets(1, 8, [0, 0], [0, 7], [1.0, -1.0])
+    lp = sp().LpProblem(1, 8, rp, ci, v, np.linspace(-1.0, 1.0, 8), np.array([-inf]), np.array([1.0]), np.zeros(8),
+                        np.full(8, 10.0))
+    with pytest.raises(RuntimeError, match="numerical"):
+        oracle.solve(lp, tolerance=TOL)
+    for solve in (sp().solve, sp().solve_stepwise):
+        with pytest.raises(sp().SolveError) as e:
+            solve(lp, sp().SolverParams(tolerance=TOL), gpu_backend)
+        assert e.value.code == 5, e.value

@@ -149,3 +149,22 @@ def test_stream_engine_solve_of_ragged_lp_matches_oracle(gpu_backend):
     assert abs(int(g.iterations) - int(ref.iterations)) <= 64
     if ref.status == "Optimal":
         oracle.check(lp, g.x, g.y).verify(2e-4)
+
+
+def test_stream_engine_stall_path_reports_and_leaves_the_context_usable(powerlaw_lp, gpu_backend):
+    """The stream engine's bounded waits, exercised without a fault: with the test knob
+    SP_TEST_STREAM_WITHHOLD (read when a solver is created) the loader never issues the
+    copies of one tile and every wait gives up after 100 µs, so the CTA that owns that
+    tile takes its stall path (no copy is in flight, nothing faults). The solve must end
+    with SP_ERR_CUDA and the stall message, and the next solve on the same context must
+    give a clean solve's bits."""
+    params = fixed_iterations(192)
+    clean = solve_with("stream", powerlaw_lp, params, gpu_backend)
+    os.environ["SP_TEST_STREAM_WITHHOLD"] = "0"
+    try:
+        with pytest.raises(sp().SolveError) as e:
+            solve_with("stream", powerlaw_lp, params, gpu_backend)
+    finally:
+        del os.environ["SP_TEST_STREAM_WITHHOLD"]
+    assert e.value.code == 1 and "did not complete within its wait limit" in str(e.value)
+    assert_identical(solve_with("stream", powerlaw_lp, params, gpu_backend), clean)

@@ -268,3 +268,4 @@ def test_netlib_quick_cupdlpx_termination(name):
 @pytest.mark.parametrize("name", SLOW)
 def test_netlib_slow(name):
     _run_netlib(name, 0)
+
