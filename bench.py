@@ -287,7 +287,8 @@ def time_form(sp, torch, lp, backend, precision, steps, warmup, dist, device):
     kern = {}
     for kid, name in ((0, "primal_pass"), (1, "dual_pass")):
         n, tot, bpl = solver.kernel_timing(kid)
-        kern[name] = {"launches_timed": n, "avg_ms": tot / max(n, 1), "bytes_per_launch": bpl}
+        kern[name] = {"launches_timed": n, "avg_ms": tot / max(n, 1), "bytes_per_launch": bpl,
+                      "gather_floor_ms": solver.gather_floor(kid, fp32=precision == sp.Precision.Mixed)}
     solver.set_timing(0)
     info = solver.info()
     out = {
@@ -357,10 +358,15 @@ def run_ours(args):
                 "traffic_source": f"profiles/ncu_traffic.txt ({dom} {wkey} {form})",
                 "bytes_per_launch": d["bytes_per_launch"], "avg_launch_ms": d["avg_ms"],
                 "launches_timed": d["launches_timed"],
+                "gather_floor": {"ms": d["gather_floor_ms"], "frac": d["gather_floor_ms"] / d["avg_ms"]
+                                 if d["avg_ms"] > 0 else None,
+                                 "what": "a kernel doing only this pass's random gathers through its own index "
+                                         "stream (no values, no epilogue); frac = its time / the pass's"},
                 "timing": "CUDA events on the library's stream around every 4th launch of the pass, in an "
                           "untimed pass of direct launches right after the timed graph replays",
                 "other": {name: {"achieved_gbs": k[name]["bytes_per_launch"] / (k[name]["avg_ms"] * 1e-3) / 1e9
                                  if k[name]["avg_ms"] > 0 else None, "avg_launch_ms": k[name]["avg_ms"],
+                                 "gather_floor_ms": k[name]["gather_floor_ms"],
                                  "traffic": profiled_traffic(name, wkey, form)}
                           for name in k if name != dom}}
 
@@ -386,8 +392,9 @@ def run_ours(args):
                   "iterations, unscaled solution back)"}
 
     # to 1e-6 relative KKT in both forms, end to end; checked outside the timing
+    # (one GPU only: with N replicas every rank would repeat the same single-GPU solves)
     tol_res = {}
-    if not args.no_tolerance:
+    if not args.no_tolerance and dist.world == 1:
         golden = oracle_golden(args)
         for prec, name in ((sp.Precision.FP64, "fp64"), (sp.Precision.Mixed, "mixed")):
             sol_t, secs, wall = to_tolerance(sp, torch, pinned, backend, prec, device, args.tolerance,
@@ -417,7 +424,7 @@ def run_ours(args):
         cpu = cpu_baseline(lp, f64["scaled"], f64["norm_estimate"])
 
     batch = None
-    if args.workload == "powerlaw" and args.scale == 1.0 and not args.no_batch:
+    if args.workload == "powerlaw" and args.scale == 1.0 and not args.no_batch and dist.world == 1:
         batch = batch_compact(sp, backend, dist, args.seed)
 
     clocks = f64["clocks"]

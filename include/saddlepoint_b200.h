@@ -231,6 +231,11 @@ double sp_solver_bytes_per_iteration(sp_solver *s);
  * out[2] dual FP64, out[3] dual FP32 (the FP32 entries apply to the mixed form). */
 enum { SP_ENGINE_TILES = 0, SP_ENGINE_STREAM = 1, SP_ENGINE_SELL = 2 };
 int sp_solver_engines(sp_solver *s, int32_t out[4]);
+/* The floor a pass's random gathers set: the average time of a kernel that does only
+ * those gathers (pass 0 primal: y through A'ᵀ's column indices; 1 dual: x̄ through A''s;
+ * fp32 != 0: the mixed form's FP32 vectors), each through the pass's own index stream,
+ * over `reps` launches after one warm-up. For reading a pass's time against. */
+int sp_solver_gather_floor(sp_solver *s, int pass, int fp32, int reps, double *ms_per_launch);
 /* Kernel launches of one epoch of check_every iterations, counted from the
  * kernel nodes of its CUDA graph (the graph is built if it does not exist yet). */
 int sp_solver_epoch_kernels(sp_solver *s, int64_t *count);

@@ -515,6 +515,13 @@ class Solver(_Handle):
         keys = ("primal_fp64", "primal_fp32", "dual_fp64", "dual_fp32")
         return {k: self.ENGINES[int(v)] for k, v in zip(keys, out)}
 
+    def gather_floor(self, kernel_id: int, fp32: bool = False, reps: int = 10) -> float:
+        """Milliseconds of a kernel doing only pass `kernel_id`'s gathers (0 primal, 1 dual)
+        through its own index stream: the floor its random gathers set."""
+        ms = C.c_double()
+        self._c(self.lib.sp_solver_gather_floor(self.h, kernel_id, int(fp32), reps, C.byref(ms)))
+        return ms.value
+
     def epoch_kernels(self) -> int:
         """Kernel launches in one epoch of check_every iterations (its graph's kernel nodes)."""
         n = C.c_int64()

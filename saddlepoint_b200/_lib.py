@@ -153,6 +153,7 @@ SIGNATURES = [
     ("sp_solver_bytes_per_iteration", dbl, [VP]),
     ("sp_solver_engines", cint, [VP, C.POINTER(C.c_int32)]),
     ("sp_solver_epoch_kernels", cint, [VP, PI64]),
+    ("sp_solver_gather_floor", cint, [VP, cint, cint, cint, PD]),
     ("sp_solver_scaled", cint, [VP, PI64, PI32, PD, PI64, PI32, PD, PD, PD, PD, PD, PD, PD, PD, PD, PD]),
     ("sp_solver_free", None, [VP]),
     ("sp_batch_create", cint, [VP, C.POINTER(Lp), cint, C.POINTER(Params), C.POINTER(VP)]),

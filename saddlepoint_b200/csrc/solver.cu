@@ -692,11 +692,19 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
         cudaStreamWaitEvent(s->aux, s->fork, 0);
         const unsigned gr = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32));
         // rows of 16+ chunks on average (the transport LP's 63): 4 chunks per batch
-        if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        if (S.piped == 1) k_sell_rows_piped<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        else if (S.piped == 2) k_sell_rows_piped<Op, 1, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        else if (S.piped == 3) k_sell_rows_piped<Op, 2, 3><<<gr, NT, 0, s->aux>>>(op, a);
+        else if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
         else k_sell_rows<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
     }
     // FP32 values: 5 CTAs per SM (0.176 ms against 0.182 at 4, with 512-row windows)
-    if constexpr (sizeof(typename Op::VT) == 4) k_sell_win<Op, 8, 5><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    if (S.early) {
+        if constexpr (sizeof(typename Op::VT) == 4) k_sell_win_early<Op, 4, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+        else if (S.early == 2) k_sell_win_early<Op, 4, 3><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+        else if (S.early == 3) k_sell_win_early<Op, 3, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+        else k_sell_win_early<Op, 4, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    } else if constexpr (sizeof(typename Op::VT) == 4) k_sell_win<Op, 8, 5><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
     else k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
     if (rows) {
         cudaEventRecord(s->join, s->aux);
@@ -715,7 +723,8 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
 // iteration's time is launch latency and tile parallelism (32 LPs of the batch workload,
 // one device solve each: 9.1 µs per iteration on tiles, 9.5 stream, 11.6 SELL).
 // SP_PASS_ENGINE=tiles|stream|sell overrides all four (large: the assignment above for a
-// problem of any size); SP_STREAM_GATHER names the stream variant.
+// problem of any size), SP_PRIMAL_ENGINE and SP_DUAL_ENGINE one pass; SP_STREAM_GATHER
+// names the stream variant.
 constexpr int64_t SMALL_NNZ = 1 << 20;
 
 int choose_engines(sp_solver *s) {
@@ -734,13 +743,20 @@ int choose_engines(sp_solver *s) {
     }
     if (eng && !strcmp(eng, "tiles")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = -1;
     if (eng && !strcmp(eng, "sell")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = ENGINE_SELL;
-    if (eng && !strcmp(eng, "stream")) {
-        int v = SV_LDG4;
-        const char *gv = getenv("SP_STREAM_GATHER");
-        for (int k = 0; gv && k < SV_COUNT; ++k)
-            if (!strcmp(gv, STREAM_VARIANT_NAMES[k])) v = k;
-        s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = v;
-    }
+    int sv = SV_LDG4;
+    if (const char *gv = getenv("SP_STREAM_GATHER"))
+        for (int k = 0; k < SV_COUNT; ++k)
+            if (!strcmp(gv, STREAM_VARIANT_NAMES[k])) sv = k;
+    if (eng && !strcmp(eng, "stream")) s->sv_p64 = s->sv_p32 = s->sv_d64 = s->sv_d32 = sv;
+    // one pass's engine alone (measurements): SP_PRIMAL_ENGINE / SP_DUAL_ENGINE = tiles|stream|sell
+    auto pick = [&](const char *name, int *v64, int *v32) {
+        const char *e = getenv(name);
+        if (!e) return;
+        const int v = !strcmp(e, "tiles") ? -1 : !strcmp(e, "sell") ? ENGINE_SELL : !strcmp(e, "stream") ? sv : -2;
+        if (v != -2) *v64 = *v32 = v;
+    };
+    pick("SP_PRIMAL_ENGINE", &s->sv_p64, &s->sv_p32);
+    pick("SP_DUAL_ENGINE", &s->sv_d64, &s->sv_d32);
     const int dev = s->ctx->device;
     int rc;
     // the SELL copies, where a pass uses them (a matrix with a row longer than a tile
@@ -748,6 +764,9 @@ int choose_engines(sp_solver *s) {
     const bool sell_p = s->sv_p64 == ENGINE_SELL || (s->mixed && s->sv_p32 == ENGINE_SELL);
     const bool sell_d = s->sv_d64 == ENGINE_SELL || (s->mixed && s->sv_d32 == ENGINE_SELL);
     if (sell_p && (rc = build_sell(s, s->AT, &s->sellAT))) return rc;
+    // kernel shapes of the primal pass on its SELL copy (measurements)
+    s->sellAT.early = getenv("SP_SELL_EARLY") ? atoi(getenv("SP_SELL_EARLY")) : 0;
+    s->sellAT.piped = getenv("SP_SELL_PIPED") ? atoi(getenv("SP_SELL_PIPED")) : 0;
     if (sell_d && (rc = build_sell(s, s->A, &s->sellA))) return rc;
     for (int *v : {&s->sv_p64, &s->sv_p32})
         if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;
@@ -1553,6 +1572,71 @@ extern "C" int sp_solver_kernel_timing(sp_solver *s, int id, int64_t *launches, 
 }
 
 extern "C" double sp_solver_bytes_per_iteration(sp_solver *s) { return s ? s->pass_bytes(0) + s->pass_bytes(1) : 0.0; }
+
+namespace sp {
+
+// The gathers of a pass and nothing else: every nonzero's entry of the gathered vector,
+// addressed through the pass's own column-index stream (coalesced, 8 loads in flight per
+// thread), summed per warp into `out` so nothing is optimised away. Its time is the floor
+// the pass's random gathers set on this GPU (no values, no epilogue, no staging).
+template <class GT>
+__global__ void __launch_bounds__(NT) k_gather_floor(const int *__restrict__ ci, int64_t nnz,
+                                                     const GT *__restrict__ gv, double *__restrict__ out) {
+    const int64_t stride = (int64_t)gridDim.x * NT;
+    int64_t k = blockIdx.x * (int64_t)NT + threadIdx.x;
+    double acc = 0.0;
+    for (; k + 7 * stride < nnz; k += 8 * stride) {
+        int c[8];
+        GT g[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) c[u] = ld_stream(ci + k + u * stride);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) g[u] = __ldg(gv + c[u]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc += double(g[u]);
+    }
+    for (; k < nnz; k += stride) acc += double(__ldg(gv + ld_stream(ci + k)));
+    acc = warp_sum_down(acc);
+    if ((threadIdx.x & 31) == 0) out[blockIdx.x * (NT / 32) + (threadIdx.x >> 5)] = acc;
+}
+
+}  // namespace sp
+
+extern "C" int sp_solver_gather_floor(sp_solver *s, int pass, int fp32, int reps, double *ms_per_launch) {
+    if (!s || pass < 0 || pass > 1 || reps < 1 || !ms_per_launch) return SP_ERR_INVALID;
+    if (fp32 && !s->mixed) return fail(SP_ERR_INVALID, "FP32 gathers exist in the mixed form only");
+    int rc = enter(s->ctx);
+    if (rc) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const DevCsr &M = pass == 0 ? s->AT : s->A;
+    if (M.nnz == 0) {
+        *ms_per_launch = 0.0;
+        return SP_OK;
+    }
+    int per_sm = 0;
+    const void *f = fp32 ? (const void *)k_gather_floor<float> : (const void *)k_gather_floor<double>;
+    SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, NT, 0));
+    const int grid = std::max(1, per_sm) * s->ctx->sms;
+    double *out = nullptr;
+    if ((rc = dalloc(&out, (int64_t)grid * (NT / 32)))) return rc;
+    EventPair ep;
+    if ((rc = ep.init())) return rc;
+    auto launch = [&] {
+        if (fp32) k_gather_floor<float><<<grid, NT, 0, st>>>(M.ci, M.nnz, pass == 0 ? s->y32 : s->xbar32, out);
+        else k_gather_floor<double><<<grid, NT, 0, st>>>(M.ci, M.nnz, pass == 0 ? s->y : s->xbar, out);
+    };
+    launch();
+    SP_CUDA_TRY(cudaEventRecord(ep.e0, st));
+    for (int r = 0; r < reps; ++r) launch();
+    SP_CUDA_TRY(cudaEventRecord(ep.e1, st));
+    SP_CUDA_TRY(cudaEventSynchronize(ep.e1));
+    float ms = 0.f;
+    SP_CUDA_TRY(cudaEventElapsedTime(&ms, ep.e0, ep.e1));
+    dfree(out, st);
+    SP_CUDA_TRY(cudaGetLastError());
+    *ms_per_launch = (double)ms / reps;
+    return SP_OK;
+}
 
 extern "C" int sp_solver_engines(sp_solver *s, int32_t out[4]) {
     if (!s || !out) return SP_ERR_INVALID;

@@ -168,3 +168,18 @@ def test_stream_engine_stall_path_reports_and_leaves_the_context_usable(powerlaw
         del os.environ["SP_TEST_STREAM_WITHHOLD"]
     assert e.value.code == 1 and "did not complete within its wait limit" in str(e.value)
     assert_identical(solve_with("stream", powerlaw_lp, params, gpu_backend), clean)
+
+
+def test_gather_floor_is_below_the_pass_time(powerlaw_lp, gpu_backend):
+    """sp_solver_gather_floor times a kernel doing only a pass's gathers; the fused pass does
+    those gathers and more, so its launch takes longer than the floor."""
+    s = sp().Solver(powerlaw_lp, fixed_iterations(10**9), gpu_backend)
+    s.run_epochs(2)
+    s.set_timing(1)
+    s.run_epochs(2)
+    s.sync()
+    for kid in (0, 1):
+        n, tot, _ = s.kernel_timing(kid)
+        floor = s.gather_floor(kid)
+        assert n > 0 and 0.0 < floor < tot / n, (kid, floor, tot / n)
+    s.close()

@@ -61,3 +61,28 @@ def test_dot_noalloc_rejects_lengths_beyond_its_scratch(gpu_backend):
     assert lib.sp_dot_noalloc(p, p, 8, C.c_void_p(out.data_ptr()), None) == SP_OK
     torch.cuda.synchronize()
     assert float(out.item()) == 8.0
+
+
+def test_dot_noalloc_at_its_maximum_length(gpu_backend):
+    """n = SP_NOALLOC_DOT_MAX_N fills every partial-sum slot of the static array. The
+    entries (1 and (k mod 7) - 3) make every partial sum an exact integer, so the result
+    equals the float64 value of the exact sum whatever the order of the additions."""
+    import torch
+
+    import saddlepoint_b200 as sp
+
+    lib = sp.library()
+    n = MAX_N
+    a = torch.ones(n, dtype=torch.float64, device="cuda")
+    b = (torch.arange(n, dtype=torch.int64, device="cuda") % 7 - 3).to(torch.float64)
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    exact = sum((k % 7) - 3 for k in range(n % 7))  # whole periods of 7 sum to zero
+    for _ in range(2):
+        rc = lib.sp_dot_noalloc(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                C.c_void_p(stream.cuda_stream))
+        assert rc == SP_OK
+        stream.synchronize()
+        assert float(out.item()) == float(exact)
+    del a, b
+    torch.cuda.empty_cache()
