@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the power-law LP's m, n and nnz by this factor (profiling runs only)")
     ap.add_argument("--tolerance", type=float, default=1e-6, help="relative KKT target of the to-tolerance solves")
-    ap.add_argument("--tolerance-limit-s", type=float, default=120.0, help="time limit of each to-tolerance solve")
+    ap.add_argument("--tolerance-limit-s", type=float, default=300.0, help="time limit of each to-tolerance solve")
     ap.add_argument("--no-tolerance", action="store_true", help="skip the solves to the tolerance")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form section of the default line")
     return ap.parse_args()
@@ -220,8 +220,9 @@ GOLDEN_FULL = os.path.join(ROOT, "tests", "golden", "powerlaw_m2000000_n4000000_
 
 
 def oracle_golden(args):
-    """The oracle's committed FP64 solve of the default workload at 1e-6 (status, iterations,
-    objective), written by tests/golden/make_scale_goldens.py; None for other workloads."""
+    """The oracle's committed fixture of the default workload (tests/golden/
+    make_scale_goldens.py): its FP64 solve at 1e-6 (status, iterations, objective) where the
+    oracle ran it to the end; None for other workloads."""
     if args.workload != "powerlaw" or args.scale != 1.0 or args.seed != 1:
         return None
     try:
@@ -408,7 +409,7 @@ def run_ours(args):
                  "dual_objective": sol_t.dual_objective}
             if dist.rank == 0:
                 r["checker"] = checker_report(lp, sol_t, args.tolerance)
-            if golden:
+            if golden and "objective" in golden:  # the oracle's full solve, where it was run to the end
                 g_obj = golden["objective"]
                 r["oracle_fp64"] = {k: golden[k] for k in ("status", "iterations", "objective", "threads")}
                 r["objective_gap_vs_oracle_fp64"] = abs(sol_t.objective - g_obj) / (1.0 + abs(g_obj))

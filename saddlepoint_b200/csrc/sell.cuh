@@ -51,8 +51,6 @@ struct SellMat {
     int64_t nrows = 0, nwin = 0, nslices = 0, slots = 0;
     int64_t nheavy = 0, nseg = 0, chunks = 0;
     bool split = false;         // rows and windows as two launches on two streams (a large pass)
-    int early = 0;              // windows by k_sell_win_early (rows mostly narrower than its batch)
-    int piped = 0;              // warp rows by k_sell_rows_piped (gathers two batches deep)
     int *ci = nullptr;          // [slots] slices
     double *v = nullptr;        // [slots]
     float *v32 = nullptr;       // [slots], mixed form
@@ -286,104 +284,6 @@ __global__ void __launch_bounds__(NT, MINB) k_sell_rows(Op op, SellArgs S) {
     if (seg < S.nseg) sell_rows_body<Op, BH>(op, S, seg);
 }
 
-// sell_rows_body with the gathers two batches deep: while batch b is summed, the gathers of
-// batch b + 1 are in flight and the index/value loads of batch b + 2 are issued, so a warp
-// keeps 2·BH chunks of gathers outstanding instead of BH. The sums are sell_rows_body's.
-template <class Op, int BH>
-__device__ __forceinline__ void sell_rows_piped_body(Op &op, const SellArgs &S, int64_t seg) {
-    using VT = typename Op::VT;
-    using GT = typename Op::GT;
-    using Pre = typename Op::Pre;
-    static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
-    constexpr bool F32 = (Op::F32 & 1u) != 0;
-    using AT = typename std::conditional<F32, float, double>::type;
-    const int lane = threadIdx.x & 31;
-    const GT *__restrict__ gv = op.gvec();
-    double part[1] = {0.0};
-    const int64_t h0 = S.segrow[seg];
-    const int nr = S.segrow[seg + 1] - (int)h0;
-    if (nr == 0) return;  // a block inside one long row
-    int row = 0;
-    int64_t bound = 0;
-    Pre pre{};
-    if (lane <= nr) bound = S.choff[h0 + lane];
-    if (lane < nr) {
-        row = S.heavy[h0 + lane];
-        pre = op.pre(row);
-    }
-    const int64_t c0 = __shfl_sync(0xffffffffu, bound, 0), c1 = __shfl_sync(0xffffffffu, bound, nr);
-    const VT *__restrict__ hv;
-    if constexpr (sizeof(VT) == 4) hv = reinterpret_cast<const VT *>(S.hv32);
-    else hv = reinterpret_cast<const VT *>(S.hv);
-    int cur = 0;
-    AT s = AT(-0.0);
-    auto finish = [&]() {
-        const AT tot = __shfl_sync(0xffffffffu, warp_sum_down(s), 0);
-        if (lane == cur) {
-            const double sum[1] = {double(tot)};
-            op.row(row, sum, part, pre);
-        }
-    };
-    const int *__restrict__ pc = S.hci + c0 * 32 + lane;
-    const VT *__restrict__ pv = hv + c0 * 32 + lane;
-    const int nch = (int)(c1 - c0);
-    int nxt = (int)(__shfl_sync(0xffffffffu, bound, 1) - c0);
-    // batch b covers chunks [b·BH, b·BH + BH): A = the batch being summed (values, gathers),
-    // B = the next (values, gathers in flight), C = the one after (indices, values loading)
-    auto load = [&](int first, int (&c)[BH], VT (&v)[BH]) {
-#pragma unroll
-        for (int u = 0; u < BH; ++u) {
-            c[u] = -1;
-            if (first + u < nch) {
-                c[u] = ld_stream(pc + 32 * (first + u));
-                v[u] = ld_stream(pv + 32 * (first + u));
-            }
-        }
-    };
-    auto gather = [&](const int (&c)[BH], GT (&g)[BH]) {
-#pragma unroll
-        for (int u = 0; u < BH; ++u)
-            if (c[u] >= 0) g[u] = __ldg(gv + c[u]);
-    };
-    int cA[BH], cB[BH], cC[BH];
-    VT vA[BH], vB[BH], vC[BH];
-    GT gA[BH], gB[BH];
-    load(0, cA, vA);
-    load(BH, cB, vB);
-    gather(cA, gA);
-    for (int ch = 0; ch < nch; ch += BH) {
-        gather(cB, gB);
-        load(ch + 2 * BH, cC, vC);
-#pragma unroll
-        for (int u = 0; u < BH; ++u) {
-            if (ch + u >= nch) break;
-            if (ch + u == nxt) {  // a warp row spans at least two chunks
-                finish();
-                ++cur;
-                nxt = (int)(__shfl_sync(0xffffffffu, bound, cur + 1) - c0);
-                s = AT(-0.0);
-            }
-            if (cA[u] >= 0) s += AT(op.mul(vA[u], gA[u]));
-        }
-#pragma unroll
-        for (int u = 0; u < BH; ++u) {
-            cA[u] = cB[u];
-            vA[u] = vB[u];
-            gA[u] = gB[u];
-            cB[u] = cC[u];
-            vB[u] = vC[u];
-        }
-    }
-    finish();
-}
-
-template <class Op, int BH, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sell_rows_piped(Op op, SellArgs S) {
-    if (!op.setup()) return;
-    const int64_t seg = (int64_t)blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
-    if (seg < S.nseg) sell_rows_piped_body<Op, BH>(op, S, seg);
-}
-
 // The short rows of window `win` of a FUSED pass (NP = 0, one gathered vector) on the SELL
 // copy, by one CTA: BS slice entries in flight per lane.
 template <class Op, int BS>
@@ -454,103 +354,6 @@ template <class Op, int BS, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_sell_win(Op op, SellArgs S) {
     if (!op.setup()) return;
     sell_win_body<Op, BS>(op, S, blockIdx.x);
-}
-
-// The short rows of window `win` with a shorter chain of dependent loads, for passes whose
-// short rows are mostly narrower than BS (the primal pass: 81 % of its rows hold 2-3
-// entries): every slice's metadata first, then the first BS entries of all of the warp's
-// slices at once, their gathers, the epilogue's row inputs while those are in flight, and
-// only then the sums; a slice wider than BS takes its other entries in batches of BS.
-// Each row's sum is the same as sell_win_body's (one thread, column order, from -0.0).
-template <class Op, int BS>
-__device__ __forceinline__ void sell_win_early_body(Op &op, const SellArgs &S, int64_t win) {
-    using VT = typename Op::VT;
-    using GT = typename Op::GT;
-    using Pre = typename Op::Pre;
-    static_assert(Op::G == 1 && Op::NP == 0, "the SELL path runs passes that gather one vector and reduce nothing");
-    constexpr bool F32 = (Op::F32 & 1u) != 0;
-    using AT = typename std::conditional<F32, float, double>::type;
-    constexpr int W = NT / 32, Q = SELL_SPW, RPT = SELL_WIN / NT;
-    __shared__ AT sums[SELL_WIN];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const GT *__restrict__ gv = op.gvec();
-    double part[1] = {0.0};
-    const VT *__restrict__ sv;
-    if constexpr (sizeof(VT) == 4) sv = reinterpret_cast<const VT *>(S.v32);
-    else sv = reinterpret_cast<const VT *>(S.v);
-    int l[Q], L[Q], pos[Q];
-    int64_t off[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const int ls = q * W + ((q & 1) ? W - 1 - warp : warp);
-        const int64_t sl = win * (SELL_WIN / 32) + ls;
-        const int64_t k = sl * 32 + lane;
-        l[q] = S.lsort[k];
-        L[q] = S.slen[sl];
-        off[q] = S.off[sl] + lane;
-        pos[q] = S.perm[k];
-    }
-    const int64_t rbase = win * SELL_WIN + threadIdx.x;
-    bool live[RPT];
-#pragma unroll
-    for (int u = 0; u < RPT; ++u) {
-        const int64_t r = rbase + u * NT;
-        live[u] = r < S.nrows && S.len[r] != SELL_HEAVY;
-    }
-    int c[Q][BS];
-    VT v[Q][BS];
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-#pragma unroll
-        for (int u = 0; u < BS; ++u)
-            if (u < l[q]) {
-                c[q][u] = ld_stream(S.ci + off[q] + 32ll * u);
-                v[q][u] = ld_stream(sv + off[q] + 32ll * u);
-            }
-    GT g[Q][BS];
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-#pragma unroll
-        for (int u = 0; u < BS; ++u)
-            if (u < l[q]) g[q][u] = __ldg(gv + c[q][u]);
-    Pre pre[RPT];
-#pragma unroll
-    for (int u = 0; u < RPT; ++u)
-        if (live[u]) pre[u] = op.pre((int)(rbase + u * NT));
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        AT s = AT(-0.0);
-#pragma unroll
-        for (int u = 0; u < BS; ++u)
-            if (u < l[q]) s += AT(op.mul(v[q][u], g[q][u]));
-        for (int j0 = BS; j0 < L[q]; j0 += BS) {
-            int cc[BS];
-            VT vv[BS];
-#pragma unroll
-            for (int u = 0; u < BS; ++u)
-                if (j0 + u < l[q]) {
-                    cc[u] = ld_stream(S.ci + off[q] + 32ll * (j0 + u));
-                    vv[u] = ld_stream(sv + off[q] + 32ll * (j0 + u));
-                }
-#pragma unroll
-            for (int u = 0; u < BS; ++u)
-                if (j0 + u < l[q]) s += AT(op.mul(vv[u], __ldg(gv + cc[u])));
-        }
-        sums[pos[q]] = s;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < RPT; ++u) {
-        if (!live[u]) continue;
-        const double sum[1] = {double(sums[threadIdx.x + u * NT])};
-        op.row((int)(rbase + u * NT), sum, part, pre[u]);
-    }
-}
-
-template <class Op, int BS, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_sell_win_early(Op op, SellArgs S) {
-    if (!op.setup()) return;
-    sell_win_early_body<Op, BS>(op, S, blockIdx.x);
 }
 
 // Both parts of a small FUSED pass in one launch: the first ceil(nseg / 8) CTAs take the

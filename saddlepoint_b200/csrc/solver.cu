@@ -692,19 +692,11 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
         cudaStreamWaitEvent(s->aux, s->fork, 0);
         const unsigned gr = (unsigned)((S.nseg + NT / 32 - 1) / (NT / 32));
         // rows of 16+ chunks on average (the transport LP's 63): 4 chunks per batch
-        if (S.piped == 1) k_sell_rows_piped<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
-        else if (S.piped == 2) k_sell_rows_piped<Op, 1, 4><<<gr, NT, 0, s->aux>>>(op, a);
-        else if (S.piped == 3) k_sell_rows_piped<Op, 2, 3><<<gr, NT, 0, s->aux>>>(op, a);
-        else if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
+        if (sizeof(typename Op::VT) == 4 || S.chunks >= 16 * S.nheavy) k_sell_rows<Op, 4, 4><<<gr, NT, 0, s->aux>>>(op, a);
         else k_sell_rows<Op, 2, 4><<<gr, NT, 0, s->aux>>>(op, a);
     }
     // FP32 values: 5 CTAs per SM (0.176 ms against 0.182 at 4, with 512-row windows)
-    if (S.early) {
-        if constexpr (sizeof(typename Op::VT) == 4) k_sell_win_early<Op, 4, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
-        else if (S.early == 2) k_sell_win_early<Op, 4, 3><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
-        else if (S.early == 3) k_sell_win_early<Op, 3, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
-        else k_sell_win_early<Op, 4, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
-    } else if constexpr (sizeof(typename Op::VT) == 4) k_sell_win<Op, 8, 5><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
+    if constexpr (sizeof(typename Op::VT) == 4) k_sell_win<Op, 8, 5><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
     else k_sell_win<Op, 8, 4><<<(unsigned)S.nwin, NT, 0, st>>>(op, a);
     if (rows) {
         cudaEventRecord(s->join, s->aux);
@@ -764,9 +756,6 @@ int choose_engines(sp_solver *s) {
     const bool sell_p = s->sv_p64 == ENGINE_SELL || (s->mixed && s->sv_p32 == ENGINE_SELL);
     const bool sell_d = s->sv_d64 == ENGINE_SELL || (s->mixed && s->sv_d32 == ENGINE_SELL);
     if (sell_p && (rc = build_sell(s, s->AT, &s->sellAT))) return rc;
-    // kernel shapes of the primal pass on its SELL copy (measurements)
-    s->sellAT.early = getenv("SP_SELL_EARLY") ? atoi(getenv("SP_SELL_EARLY")) : 0;
-    s->sellAT.piped = getenv("SP_SELL_PIPED") ? atoi(getenv("SP_SELL_PIPED")) : 0;
     if (sell_d && (rc = build_sell(s, s->A, &s->sellA))) return rc;
     for (int *v : {&s->sv_p64, &s->sv_p32})
         if (*v == ENGINE_SELL && !s->sellAT.ok) *v = -1;

@@ -15,7 +15,9 @@ library nor a GPU. Every fixture records:
     objective, dual objective, ‖A'‖₂ estimate, seconds, threads, and its whole check
     trace (total, restart decision, k after the check, ω, residual);
   * where the case asks for it, the trace of a run stopped after a fixed number of
-    iterations (every check of the first 640 iterations, say).
+    iterations (every check of the first 640 iterations, say), written before the full
+    solve starts: the oracle needs hours for the full solve of the largest LP, and the
+    fixture of the fixed run stands on its own if that solve is cut short.
 
 The oracle's reductions above 32768 elements are chunked by its thread count, so its
 results depend (at rounding level) on --threads, which the fixture records.
@@ -40,7 +42,7 @@ if ROOT not in sys.path:
 CASES = {
     "powerlaw_m200000_n400000_nnz3000000_seed3": ("powerlaw", (3, 200_000, 400_000, 3_000_000), 1e-6, 640),
     "transport_300x300_seed5": ("transport", (5, 300, 300), 1e-6, 640),
-    "powerlaw_m2000000_n4000000_nnz40000000_seed1": ("powerlaw", (1, 2_000_000, 4_000_000, 40_000_000), 1e-6, 0),
+    "powerlaw_m2000000_n4000000_nnz40000000_seed1": ("powerlaw", (1, 2_000_000, 4_000_000, 40_000_000), 1e-6, 6400),
 }
 
 
@@ -70,7 +72,9 @@ def trace_rows(trace):
     return [[t["total"], int(t["restarted"]), t["k_after"], t["omega"], t["residual"]] for t in trace]
 
 
-def make(name: str, threads: int) -> dict:
+def make(name: str, threads: int, path: str) -> dict:
+    """Writes the fixture to `path`: first with the fixed run alone (so a long full solve
+    that is cut short still leaves it), then again with the full solve."""
     import oracle
 
     kind, args, tol, fixed = CASES[name]
@@ -79,9 +83,14 @@ def make(name: str, threads: int) -> dict:
     out = {"name": name, "generator": kind, "args": list(args), "nrows": lp.nrows, "ncols": lp.ncols,
            "nnz": lp.nnz, "fingerprint": fingerprint(lp), "tolerance": tol, "threads": oracle.get_threads()}
     if fixed:
+        t0 = time.time()
         r = oracle.solve(lp, tolerance=tol, max_iterations=fixed)
         out["fixed"] = {"max_iterations": fixed, "status": r.status, "iterations": r.iterations,
+                        "objective": r.objective, "norm_estimate": r.norm_estimate, "seconds": time.time() - t0,
                         "trace": trace_rows(r.trace)}
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1)
+        print(f"{name}: fixed run of {fixed} iterations written", flush=True)
     t0 = time.time()
     r = oracle.solve(lp, tolerance=tol)
     out.update(status=r.status, iterations=r.iterations, restarts=r.restarts, objective=r.objective,
@@ -99,8 +108,8 @@ def main() -> None:
     ap.add_argument("cases", nargs="*", default=list(CASES))
     a = ap.parse_args()
     for name in a.cases:
-        res = make(name, a.threads)
         path = os.path.join(HERE, f"{name}.json")
+        res = make(name, a.threads, path)
         with open(path, "w") as f:
             json.dump(res, f, indent=1)
         print(f"{name}: {res['status']} in {res['iterations']} iterations, objective {res['objective']:.12g}, "
