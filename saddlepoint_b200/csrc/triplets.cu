@@ -1,13 +1,17 @@
 // triplets.cu — CsrMatrix::from_triplets (crates/saddlepoint-core/src/problem.rs:33-77) on
 // the GPU, for loading large problems.
 //
-// The host rule (and the oracle's): entries grouped by row in input order, each row's
-// entries stably sorted by column, runs of one column summed in that order (the first value,
-// then += each next), sums that are exactly zero dropped. Here: one stable radix sort of the
-// key row·ncols + col (a radix sort keeps input order among equal keys, so every run comes
-// out in input order), a flag at the head of each run, one thread per run summing it in
-// order, a compaction of the non-zero sums, and each row's start found by a binary search
-// over the sorted keys. Same entries, same order, same bits as the host rule.
+// This library's rule (and the oracle's): entries grouped by row in input order, each row's
+// entries stably sorted by column, runs of one (row, column) summed in input order (the
+// first value, then += each next), sums that are exactly zero dropped. The reference sorts
+// each row with sort_unstable_by_key (problem.rs:60), which leaves the order of repeated
+// (row, column) entries unspecified; the two rules agree bit for bit except where a run of
+// three or more repeats of one (row, column) rounds differently in another order. Here: one
+// stable radix sort of the key row·ncols + col (a radix sort keeps input order among equal
+// keys, so every run comes out in input order), a flag at the head of each run, one thread
+// per run summing it in order, a compaction of the non-zero sums, and each row's start found
+// by a binary search over the sorted keys. Same entries, same order, same bits as the
+// library's host rule.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_select.cuh>
 #include <thrust/iterator/counting_iterator.h>
