@@ -269,3 +269,26 @@ def test_netlib_quick_cupdlpx_termination(name):
 def test_netlib_slow(name):
     _run_netlib(name, 0)
 
+
+
+def test_scale_fixtures_match_their_generated_lps():
+    """tests/golden/make_scale_goldens.py's fixtures were computed on the LPs the seeded
+    generators still build (SHA-256 of the arrays), and the oracle's answers pass its own
+    checker at twice the fixture's tolerance."""
+    import json
+    import sys
+
+    from conftest import GOLDEN
+
+    sys.path.insert(0, GOLDEN)
+    from make_scale_goldens import fingerprint
+
+    for name in ("powerlaw_m200000_n400000_nnz3000000_seed3", "transport_300x300_seed5"):
+        with open(os.path.join(GOLDEN, f"{name}.json")) as f:
+            g = json.load(f)
+        gen = oracle.generate_powerlaw_lp if g["generator"] == "powerlaw" else oracle.generate_transport_lp
+        lp = gen(*g["args"])
+        assert (lp.nrows, lp.ncols, lp.nnz) == (g["nrows"], g["ncols"], g["nnz"])
+        assert fingerprint(lp) == g["fingerprint"]
+        assert g["status"] == "Optimal" and max(g["checker"].values()) <= 2.0 * g["tolerance"]
+        assert g["fixed"]["iterations"] == g["fixed"]["max_iterations"] == 640
