@@ -373,6 +373,31 @@ int sp_csr_from_triplets(sp_ctx *ctx, int64_t nrows, int64_t ncols, int64_t ntri
                          const int64_t *cols, const double *vals, sp_csr *out);
 void sp_csr_release(sp_csr *m);
 
+/* ========================================================================
+ * Part 6 — presolve. The reference's path has none; cuPDLPx, which the reference's
+ * benchmark compares against, presolves (bench/README.md:1-6). Host code.
+ * ======================================================================== */
+
+typedef struct sp_presolve sp_presolve;
+
+/* Exact reductions of `lp` (the reference's minimisation form), applied until none
+ * applies: empty rows dropped, singleton rows turned into column bounds, fixed columns
+ * substituted into the row bounds and the objective constant, empty columns set to the
+ * bound their cost points at. `reduced` receives the remaining LP (arrays owned by the
+ * presolve object, valid until sp_presolve_free); *status is -1 when the reduced LP is to
+ * be solved, SP_STATUS_PRIMAL_INFEASIBLE or SP_STATUS_DUAL_INFEASIBLE when presolve proved
+ * it, SP_STATUS_OPTIMAL when no column is left (postsolve with null reduced vectors). */
+int sp_presolve_create(const sp_lp *lp, sp_lp *reduced, sp_presolve **out, int *status);
+/* Maps the reduced problem's solution (x_red, y_red) back to the original problem's n and
+ * m entries: removed columns take their values; removed rows take the duals that make the
+ * original KKT conditions hold as the reduced ones do (a singleton row carries the part of
+ * its column's reduced cost that the bound it implied absorbs). */
+int sp_presolve_postsolve(const sp_presolve *p, const double *x_red, const double *y_red, double *x, double *y);
+/* Rows and columns removed: counts[0] empty rows, [1] singleton rows, [2] fixed
+ * columns, [3] empty columns. */
+int sp_presolve_counts(const sp_presolve *p, int64_t counts[4]);
+void sp_presolve_free(sp_presolve *p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,7 @@ __all__ = [
     "BackendError", "SolveError", "Status", "Termination", "Precision", "LpProblem", "ScaledProblem",
     "SolverParams", "Solution", "CudaBackend", "Solver", "solve", "solve_stepwise", "BatchSolver", "Server",
     "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library", "read_mps", "MpsError",
-    "csr_from_triplets",
+    "csr_from_triplets", "presolve", "Presolved", "solve_presolved",
 ]
 
 
@@ -678,6 +678,83 @@ def generate_transport_lp(seed: int, supplies: int = 2000, demands: int = 2000) 
     """Transportation LP: supplies × demands arcs, integer supplies/demands, costs U{1..100}."""
     g = L.GenParams(kind=2, seed=seed, supplies=supplies, demands=demands)
     return _generate(g, f"transport_{supplies}x{demands}_s{seed}")
+
+
+# ------------------------------------------------------------------ presolve
+
+class Presolved:
+    """The result of presolve(): the reduced LP to solve (``reduced``), the status presolve
+    proved on its own (``status``, None when the reduced LP is to be solved), the rows and
+    columns it removed (``counts``), and postsolve()."""
+
+    def __init__(self, problem: LpProblem):
+        lib = library()
+        self._view = _LpView(problem)
+        self.problem = problem
+        out = L.Lp()
+        h = C.c_void_p()
+        st = C.c_int()
+        rc = lib.sp_presolve_create(C.byref(self._view.s), C.byref(out), C.byref(h), C.byref(st))
+        if rc != L.SP_OK:
+            raise BackendError(rc, "presolve rejected the problem")
+        self.h = h
+        m, n, nnz = out.a.nrows, out.a.ncols, out.a.nnz
+
+        def arr(ptr, k, dt):
+            return np.ctypeslib.as_array(ptr, shape=(k,)).astype(dt, copy=True) if k else np.zeros(0, dt)
+
+        self.reduced = LpProblem(m, n, arr(out.a.row_ptr, m + 1, np.int64), arr(out.a.col_idx, nnz, np.int32),
+                                 arr(out.a.values, nnz, np.float64), arr(out.c, n, np.float64),
+                                 arr(out.lc, m, np.float64), arr(out.uc, m, np.float64), arr(out.lv, n, np.float64),
+                                 arr(out.uv, n, np.float64), out.c0, bool(out.maximize), problem.name)
+        self.status = None if st.value < 0 else Status(st.value)
+        cnt = (C.c_int64 * 4)()
+        lib.sp_presolve_counts(h, cnt)
+        self.counts = dict(zip(("empty_rows", "singleton_rows", "fixed_cols", "empty_cols"), (int(v) for v in cnt)))
+
+    def postsolve(self, x_red, y_red):
+        """(x, y) of the original problem from the reduced problem's solution."""
+        xr, yr = _f64(x_red), _f64(y_red)
+        x, y = np.empty(self.problem.ncols), np.empty(self.problem.nrows)
+        rc = library().sp_presolve_postsolve(self.h, _pd(xr) if len(xr) else None, _pd(yr) if len(yr) else None,
+                                             _pd(x), _pd(y))
+        if rc != L.SP_OK:
+            raise BackendError(rc, "postsolve: the vectors do not fit the reduced problem")
+        return x, y
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().sp_presolve_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def presolve(problem) -> Presolved:
+    """Exact reductions before the solve (empty and singleton rows, fixed and empty columns),
+    host code; solve ``.reduced`` and map its answer back with ``.postsolve``."""
+    return Presolved(LpProblem.from_any(problem))
+
+
+def solve_presolved(problem, params: Optional[SolverParams] = None, backend: Optional[CudaBackend] = None) -> Solution:
+    """presolve(), the device-resident solve of the reduced LP, postsolve(): the answer in the
+    original problem's space (residuals and iteration counts are the reduced solve's)."""
+    p = LpProblem.from_any(problem)
+    pre = presolve(p)
+    try:
+        if pre.status is not None:
+            x, y = pre.postsolve(np.zeros(0), np.zeros(0)) if pre.status == Status.Optimal else (
+                np.zeros(p.ncols), np.zeros(p.nrows))
+            obj = p.objective(x)
+            return Solution(pre.status, x, y, obj, obj, 0.0, 0.0, 0.0, 0, 0, 0.0)
+        s = solve(pre.reduced, params, backend)
+        x, y = pre.postsolve(s.x, s.y)
+        return Solution(s.status, x, y, s.objective, s.dual_objective, s.primal_residual, s.dual_residual, s.gap,
+                        s.iterations, s.restarts, s.solve_time, s.setup_time, s.norm_estimate,
+                        s.fp64_from_iteration)
+    finally:
+        pre.close()
 
 
 from .batch import BatchSolver, Server  # noqa: E402  (after the core types)

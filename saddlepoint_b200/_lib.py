@@ -171,6 +171,10 @@ SIGNATURES = [
     ("sp_read_mps", cint, [C.c_char_p, C.c_size_t, C.POINTER(Lp), C.POINTER(i64), C.c_char_p, C.c_size_t]),
     ("sp_csr_from_triplets", cint, [VP, i64, i64, i64, PI64, PI64, PD, C.POINTER(Csr)]),
     ("sp_csr_release", None, [C.POINTER(Csr)]),
+    ("sp_presolve_create", cint, [C.POINTER(Lp), C.POINTER(Lp), C.POINTER(VP), C.POINTER(cint)]),
+    ("sp_presolve_postsolve", cint, [VP, PD, PD, PD, PD]),
+    ("sp_presolve_counts", cint, [VP, PI64]),
+    ("sp_presolve_free", None, [VP]),
 ]
 
 _lib = None
