@@ -711,6 +711,16 @@ def run_serve(args):
             th.join()
         wall = time.time() - t0
         srv.close()
+        # results that are neither Optimal nor the iteration cap, solved again alone (untimed)
+        params = sp.SolverParams(tolerance=1e-6, max_iterations=200_000, precision=prec)
+        alone = {}
+        for r in results:
+            if r.status not in (0, 3):
+                try:
+                    a = sp.solve(lps[index[r.id]], params, backend)
+                    alone[r.id] = {"status": int(a.status), "iterations": int(a.iterations)}
+                except sp.BackendError as e:
+                    alone[r.id] = {"error": str(e)}
         ok = [r for r in results if r.status == 0]
         lat = np.array([r.total_s for r in ok]) if ok else np.array([float("nan")])
         lat_all = np.array([r.total_s for r in results])
@@ -721,7 +731,9 @@ def run_serve(args):
                        "not_optimal_requests": sorted(
                            ({"index": index[r.id], "lp_seed": specs[index[r.id]][0], "nrows": specs[index[r.id]][1],
                              "ncols": specs[index[r.id]][2], "status": int(r.status), "iterations": int(r.iterations),
-                             "rel_primal": r.primal_residual, "rel_dual": r.dual_residual}
+                             "primal_residual": r.primal_residual, "dual_residual": r.dual_residual,
+                             "path": r.path, "error": r.error, "message": r.message,
+                             "alone": alone.get(r.id)}
                             for r in results if r.status != 0), key=lambda d: d["index"]),
                        "p50_all_s": float(np.percentile(lat_all, 50)),
                        "queue_p50_s": float(np.median([r.queue_s for r in results])), "clocks": clk.summary()}

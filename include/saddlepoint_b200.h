@@ -292,6 +292,9 @@ typedef struct {
     uint64_t iterations;
     double queue_s, solve_s, total_s; /* waiting for admission, on the device, submit to result */
     int64_t footprint_bytes;
+    int error;            /* SP_OK, or the SP_ERR_* code of a failed solve (status is then -1) */
+    int path;             /* 0: a solve slot, 1: the batched kernel */
+    char message[160];    /* the failed solve's error text */
 } sp_server_result;
 
 int sp_server_create(sp_ctx *ctx, const sp_server_config *cfg, const sp_solver_params *params, sp_server **out);

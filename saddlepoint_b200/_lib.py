@@ -104,7 +104,7 @@ class ServerResult(C.Structure):
     _fields_ = [
         ("id", i64), ("status", cint), ("objective", dbl), ("dual_objective", dbl), ("primal_residual", dbl),
         ("dual_residual", dbl), ("gap", dbl), ("iterations", u64), ("queue_s", dbl), ("solve_s", dbl),
-        ("total_s", dbl), ("footprint_bytes", i64),
+        ("total_s", dbl), ("footprint_bytes", i64), ("error", cint), ("path", cint), ("message", C.c_char * 160),
     ]
 
 

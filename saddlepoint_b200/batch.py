@@ -105,6 +105,9 @@ class ServerResult:
     footprint_bytes: int
     x: np.ndarray
     y: np.ndarray
+    error: int = 0        # SP_OK, or the SP_ERR_* code of a failed solve
+    path: str = "slot"    # "slot" (a device-resident solve) or "batch" (the batched kernel)
+    message: str = ""     # the failed solve's error text
 
 
 class Server:
@@ -151,7 +154,8 @@ class Server:
         n, m = self._shapes.pop(r.id)
         return ServerResult(r.id, r.status if rc == 0 else -1, r.objective, r.dual_objective, r.primal_residual,
                             r.dual_residual, r.gap, int(r.iterations), r.queue_s, r.solve_s, r.total_s,
-                            int(r.footprint_bytes), x[:n].copy(), y[:m].copy())
+                            int(r.footprint_bytes), x[:n].copy(), y[:m].copy(), int(r.error) or rc,
+                            "batch" if r.path == 1 else "slot", r.message.decode(errors="replace"))
 
     def close(self):
         self._handle.close()

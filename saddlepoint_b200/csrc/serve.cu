@@ -14,6 +14,7 @@
 // A request's kernels never read another request's memory and each solve is
 // deterministic, so a result is the same alone and in any mix.
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -134,6 +135,9 @@ struct sp_server {
             r->y.assign(r->lp.a.nrows, 0.0);
             r->error = sp_solve(ctx, &r->lp, &params, r->x.data(), r->y.data(), &info);
             r->res.status = r->error ? -1 : info.status;
+            r->res.error = r->error;
+            r->res.path = 0;
+            if (r->error) snprintf(r->res.message, sizeof r->res.message, "%s", sp_ctx_last_error(ctx));
             r->res.objective = info.objective;
             r->res.dual_objective = info.dual_objective;
             r->res.primal_residual = info.primal_residual;
@@ -170,6 +174,9 @@ struct sp_server {
                 if (!rc) rc = sp_batch_download(b, (int)i, r->x.data(), r->y.data());
                 r->error = rc;
                 r->res.status = rc ? -1 : res[i].status;
+                r->res.error = rc;
+                r->res.path = 1;
+                if (rc) snprintf(r->res.message, sizeof r->res.message, "%s", sp_ctx_last_error(batch_ctx));
                 r->res.objective = res[i].objective;
                 r->res.dual_objective = res[i].dual_objective;
                 r->res.primal_residual = res[i].primal_residual;
