@@ -548,6 +548,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
     dp.termination = P.termination;
     dp.mixed = b->mixed;
     dp.mixed_switch_tolerance = P.mixed_switch_tolerance;
+    dp.mixed_stall_checks = MIXED_STALL_CHECKS;
     dp.bound_objective_rescaling = P.bound_objective_rescaling;
     A.base = dp;
     A.power_iterations = P.power_iterations;

@@ -98,6 +98,7 @@ struct DevParams {
     double pid_kp, pid_ki, pid_kd, pid_discount;
     int termination, mixed;
     double mixed_switch_tolerance;
+    int mixed_stall_checks;  // checks without a 10 % gain after which the mixed form moves to FP64
     double b_norm, c_norm, c0, obj_factor, eta;
     int bound_objective_rescaling;
 };

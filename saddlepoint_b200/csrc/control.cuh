@@ -153,7 +153,7 @@ __device__ __forceinline__ void check_decide(DevState *st, const DevParams *p, c
         } else {
             st->mx_since += 1;
         }
-        if (rel < p->mixed_switch_tolerance || st->mx_since >= MIXED_STALL_CHECKS) {
+        if (rel < p->mixed_switch_tolerance || st->mx_since >= p->mixed_stall_checks) {
             st->fp64 = 1;
             st->fp64_from = total + 1;
         }

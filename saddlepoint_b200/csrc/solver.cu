@@ -1336,6 +1336,8 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     dp.termination = P.termination;
     dp.mixed = s->mixed;
     dp.mixed_switch_tolerance = P.mixed_switch_tolerance;
+    dp.mixed_stall_checks = MIXED_STALL_CHECKS;
+    if (const char *e = getenv("SP_MIXED_STALL_CHECKS")) dp.mixed_stall_checks = std::max(1, atoi(e));
     dp.b_norm = s->b_norm;
     dp.c_norm = s->c_norm;
     dp.c0 = s->c0;
