@@ -1112,17 +1112,23 @@ int transpose_on_device(sp_solver *s) {
     for (void *b : {(void *)row_of, (void *)keys_out, (void *)perm_in, (void *)perm_out, tmp}) dfree(b, st);
     // tile plan of A'ᵀ from its row pointers
     std::vector<int> rp32(n + 1);
-    SP_CUDA_TRY(cudaMemcpy(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    SP_CUDA_TRY(cudaMemcpyAsync(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
     std::vector<int64_t> rp64(rp32.begin(), rp32.end());
     std::vector<Tile> tiles = build_tiles(rp64.data(), n);
     T.ntiles = (int)tiles.size();
     T.nlong = count_long_tiles(tiles);
+    // Memory from the stream-ordered pool is ours only in the order of `st` (the pool may hand
+    // out memory whose previous owner, on another stream, is still running, with a wait
+    // for it inserted into `st`): every copy into it goes through `st`, never through the
+    // legacy stream of a synchronous cudaMemcpy.
     if ((rc = dmalloc((void **)&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)))) return rc;
     if (!tiles.empty())
-        SP_CUDA_TRY(cudaMemcpy(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice));
+        SP_CUDA_TRY(cudaMemcpyAsync(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, st));
     const std::vector<uint16_t> sched = build_schedule(rp64.data(), n, tiles);
     if ((rc = dalloc(&T.sched, n))) return rc;
-    if (n) SP_CUDA_TRY(cudaMemcpy(T.sched, sched.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    if (n) SP_CUDA_TRY(cudaMemcpyAsync(T.sched, sched.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice, st));
+    SP_CUDA_TRY(cudaStreamSynchronize(st));  // the host vectors end here
     return SP_OK;
 }
 
@@ -1288,8 +1294,9 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
         return cleanup(rc);
     if ((rc = scale_on_device(s, lp))) return cleanup(rc);
     double hn[4], hs[2];
-    SP_CUDA_TRY(cudaMemcpy(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost));
-    SP_CUDA_TRY(cudaMemcpy(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost));
+    SP_CUDA_TRY(cudaMemcpyAsync(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost, ctx->stream));
+    SP_CUDA_TRY(cudaMemcpyAsync(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+    SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     s->b_norm = hn[2];
     s->c_norm = hn[3];
     s->bound_scale = hs[0];
@@ -1344,7 +1351,8 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     dp.obj_factor = 1.0 / (s->bound_scale * s->obj_scale);  // scaling.rs:134-136
     dp.eta = P.step_size_factor / s->norm_est;
     dp.bound_objective_rescaling = P.bound_objective_rescaling;
-    SP_CUDA_TRY(cudaMemcpy(s->d_prm, &dp, sizeof dp, cudaMemcpyHostToDevice));
+    SP_CUDA_TRY(cudaMemcpyAsync(s->d_prm, &dp, sizeof dp, cudaMemcpyHostToDevice, ctx->stream));
+    SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if ((rc = sp_solver_reset(s))) return cleanup(rc);
     s->setup_s = now_s() - t0;
     *out = s;
