@@ -199,3 +199,30 @@ def test_server_admits_within_budget(gpu_backend):
     assert [r.id for r in rs] == [1, 2, 3]
     # admitted one after another: each waits for the previous to finish
     assert rs[1].queue_s >= rs[0].solve_s * 0.5 and rs[2].queue_s >= rs[1].queue_s
+
+
+def test_server_under_load_matches_solo_solves(gpu_backend):
+    """Twelve requests of 0.2M-3M nonzeros (the larger ones on the stream and SELL engines)
+    on eight concurrent slots, their set-ups and epochs overlapping and their device memory
+    handed back and forth through the stream-ordered pool: every result has the bits of the
+    same LP solved alone."""
+    rng = np.random.default_rng(17)
+    lps = []
+    for i in range(12):
+        n = int(np.exp(rng.uniform(np.log(4e4), np.log(6e5))))
+        lps.append(sp().generate_random_lp(700 + i, n // 2, n, (5, 5)))
+    params = sp().SolverParams(tolerance=TOL, max_iterations=1280)
+    srv = sp().Server(budget_bytes=100e9, max_inflight=8, batch_max_nnz=0, params=params, backend=gpu_backend)
+    ids = [srv.submit(lp) for lp in lps]
+    got = {}
+    while len(got) < len(lps):
+        r = srv.poll(timeout=120.0)
+        assert r is not None, "server stalled"
+        got[r.id] = r
+    srv.close()
+    for rid, lp in zip(ids, lps):
+        r = got[rid]
+        solo = sp().solve(lp, params, gpu_backend)
+        assert r.error == 0, r.message
+        assert r.status == int(solo.status) and r.iterations == solo.iterations
+        assert np.array_equal(r.x, solo.x) and np.array_equal(r.y, solo.y)
