@@ -64,3 +64,18 @@ def test_reference_arm_under_two_ranks_prints_one_line():
     line = lines[0]
     assert line["impl"] == "reference" and line["value"] > 0 and line["n_gpus"] == 2
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["value"] == line["value"]
+
+
+def test_reference_arm_never_loads_the_library():
+    """The reference arm builds its LP with the oracle's copy of the generators and times the
+    oracle: the CUDA library is never mapped into its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--scale', '0.0005', '--steps', '1', "
+            "'--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "m = open('/proc/self/maps').read(); print('MAPS', 'libsaddlepoint_b200' in m, 'libsp_oracle' in m)")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", PYTHONPATH=ROOT)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    maps = [l for l in r.stdout.splitlines() if l.startswith("MAPS")]
+    assert maps == ["MAPS False True"], r.stdout
+    line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][0])
+    assert line["config"]["workload"] == "single large LP, power-law columns" and "parallelism" not in line["config"]
