@@ -484,16 +484,22 @@ enum StreamVariant : int {
     SV_LDG4_DEEP,  // ... with as many slots as fit
     SV_LDG8B16,    // 8 warps, 16 loads in flight per lane
     SV_CP4,        // 4 cp.async gatherer warps
+    SV_LDG8_DEEP,  // 8 warps, 8 loads in flight per lane, as many slots as fit
+    SV_LDG6_DEEP,  // 6 warps, 8 loads, as many slots as fit
+    SV_LDG4B16_DEEP,  // 4 warps, 16 loads, as many slots as fit
+    SV_LDG4_PAIR,  // 4 warps, 8 loads, 2 slots, two CTAs per SM
+    SV_LDG6_PAIR,  // 6 warps, 8 loads, 2 slots, two CTAs per SM
     SV_COUNT
 };
-constexpr const char *STREAM_VARIANT_NAMES[SV_COUNT] = {"ldg4", "ldg4deep", "ldg8b16", "cp4"};
+constexpr const char *STREAM_VARIANT_NAMES[SV_COUNT] = {"ldg4", "ldg4deep", "ldg8b16", "cp4", "ldg8deep", "ldg6deep",
+                                                        "ldg4b16deep", "ldg4pair", "ldg6pair"};
 
 template <class Op>
 struct StreamKernel {
-    template <bool LDG, bool DEEP>
+    template <bool LDG, int DEEP>
     static constexpr size_t smem_of() { return StreamLayout<Op, !LDG, DEEP>::total; }
     static std::atomic<int> ready[64];
-    template <int GW, bool LDG, int B, bool DEEP>
+    template <int GW, bool LDG, int B, int DEEP>
     static int prepare_one() {
         constexpr size_t smem = smem_of<LDG, DEEP>();
         auto *f = k_stream<Op, GW, LDG, B, DEEP>;
@@ -508,25 +514,34 @@ struct StreamKernel {
         if (dev < 0 || dev >= 64) return fail(SP_ERR_INVALID, "device ordinal out of range");
         if (ready[dev].load()) return SP_OK;
         int rc;
-        if ((rc = prepare_one<4, true, 8, false>()) || (rc = prepare_one<4, true, 8, true>()) ||
-            (rc = prepare_one<8, true, 16, false>()) || (rc = prepare_one<4, false, 1, false>()))
+        if ((rc = prepare_one<4, true, 8, SLOTS_FEW>()) || (rc = prepare_one<4, true, 8, SLOTS_DEEP>()) ||
+            (rc = prepare_one<8, true, 16, SLOTS_FEW>()) || (rc = prepare_one<4, false, 1, SLOTS_FEW>()) ||
+            (rc = prepare_one<8, true, 8, SLOTS_DEEP>()) || (rc = prepare_one<6, true, 8, SLOTS_DEEP>()) ||
+            (rc = prepare_one<4, true, 16, SLOTS_DEEP>()) || (rc = prepare_one<4, true, 8, SLOTS_PAIR>()) ||
+            (rc = prepare_one<6, true, 8, SLOTS_PAIR>()))
             return rc;
         ready[dev].store(1);
         return SP_OK;
     }
-    template <int GW, bool LDG, int B, bool DEEP>
+    template <int GW, bool LDG, int B, int DEEP>
     static void go(int grid, const DevCsr &M, cudaStream_t st, const Op &op, const StreamTrial &tr) {
-        k_stream<Op, GW, LDG, B, DEEP><<<grid, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op, tr);
+        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)grid * stream_ctas_per_sm(DEEP), M.ntiles));
+        k_stream<Op, GW, LDG, B, DEEP><<<g, stream_threads(GW), smem_of<LDG, DEEP>(), st>>>(M.ntiles, M.nlong, op, tr);
     }
     static void launch(const sp_solver *s, const DevCsr &M, cudaStream_t st, const Op &op, int variant) {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(s->ctx->sms, M.ntiles));
         StreamTrial tr = s->trial;
         if (tr.withhold >= 0) tr.withhold += M.nlong;  // the knob counts the tiles after the long rows
         switch (variant) {
-        case SV_LDG4: go<4, true, 8, false>(grid, M, st, op, tr); break;
-        case SV_LDG4_DEEP: go<4, true, 8, true>(grid, M, st, op, tr); break;
-        case SV_LDG8B16: go<8, true, 16, false>(grid, M, st, op, tr); break;
-        default: go<4, false, 1, false>(grid, M, st, op, tr); break;
+        case SV_LDG4: go<4, true, 8, SLOTS_FEW>(grid, M, st, op, tr); break;
+        case SV_LDG4_DEEP: go<4, true, 8, SLOTS_DEEP>(grid, M, st, op, tr); break;
+        case SV_LDG8B16: go<8, true, 16, SLOTS_FEW>(grid, M, st, op, tr); break;
+        case SV_LDG8_DEEP: go<8, true, 8, SLOTS_DEEP>(grid, M, st, op, tr); break;
+        case SV_LDG6_DEEP: go<6, true, 8, SLOTS_DEEP>(grid, M, st, op, tr); break;
+        case SV_LDG4B16_DEEP: go<4, true, 16, SLOTS_DEEP>(grid, M, st, op, tr); break;
+        case SV_LDG4_PAIR: go<4, true, 8, SLOTS_PAIR>(grid, M, st, op, tr); break;
+        case SV_LDG6_PAIR: go<6, true, 8, SLOTS_PAIR>(grid, M, st, op, tr); break;
+        default: go<4, false, 1, SLOTS_FEW>(grid, M, st, op, tr); break;
         }
     }
 };

@@ -124,13 +124,18 @@ constexpr int stream_threads(int gw) { return NT + 32 + 32 * gw; }
 // Shared memory of one op: S slots of [column indices | values | row pointers |
 // gathered entries | row schedule | row inputs], scratch of the long-row tree, 3·S
 // mbarriers, the abort flag. Register gatherers (GREG = false) write each product
-// v·g over its value, so their slots have no gathered-entry region. DEEP: as many
+// v·g over its value, so their slots have no gathered-entry region. SLOTS_DEEP: as many
 // slots as fit in the 227 KB a CTA may have (at most 6); otherwise 3 for FP64 ops
 // and 4 for FP32 ones, which leaves part of the SM's 256 KB of L1/shared memory to
 // the L1 cache that the gathers hit.
 constexpr size_t STREAM_SMEM_MAX = 232448;
 
-template <class Op, bool GREG, bool DEEP>
+// Slot modes: SLOTS_FEW (3 FP64 / 4 FP32 slots, one CTA per SM), SLOTS_DEEP (as many as fit,
+// one CTA per SM), SLOTS_PAIR (2 slots, two CTAs per SM).
+enum : int { SLOTS_FEW = 0, SLOTS_DEEP = 1, SLOTS_PAIR = 2 };
+constexpr int stream_ctas_per_sm(int mode) { return mode == SLOTS_PAIR ? 2 : 1; }
+
+template <class Op, bool GREG, int DEEP>
 struct StreamLayout {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
@@ -155,7 +160,7 @@ struct StreamLayout {
     static constexpr size_t slot = pre_off + pre_bytes;
     static constexpr size_t fixed = sizeof(double) * (NT / 32) + 3 * 6 * sizeof(unsigned long long) + 16;
     static constexpr int S_FIT = (int)((STREAM_SMEM_MAX - fixed) / slot) < 6 ? (int)((STREAM_SMEM_MAX - fixed) / slot) : 6;
-    static constexpr int S = DEEP ? S_FIT : (sizeof(VT) == 4 ? 4 : 3);
+    static constexpr int S = DEEP == SLOTS_DEEP ? S_FIT : DEEP == SLOTS_PAIR ? 2 : (sizeof(VT) == 4 ? 4 : 3);
     static_assert(S >= 2, "at least two slots");
     static constexpr size_t red_off = S * slot;
     static constexpr size_t bar_off = red_off + sizeof(double) * (NT / 32);
@@ -239,7 +244,7 @@ __device__ __forceinline__ void consumer_long_row(Op &op, double *sh, int tile) 
 // GW gatherer warps; LDG: gathers through registers (B loads in flight per lane,
 // then the products stored over the values and a plain arrive) instead of cp.async;
 // DEEP: the slot count (StreamLayout).
-template <int GW, bool LDG, int B, bool DEEP, class Op>
+template <int GW, bool LDG, int B, int DEEP, class Op>
 __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntiles, int nlong, const StreamTrial tr) {
     using VT = typename Op::VT;
     using GT = typename Op::GT;
@@ -416,8 +421,8 @@ __device__ __forceinline__ void stream_run(Op &op, unsigned char *smem, int ntil
 // Runs the pass `op` if its setup() accepts this launch (a uniform choice: it
 // depends only on the device state). One CTA of stream_threads(GW) per SM, with
 // StreamLayout<Op, !LDG, DEEP>::total bytes of dynamic shared memory.
-template <class Op, int GW, bool LDG, int B, bool DEEP>
-__global__ void __launch_bounds__(stream_threads(GW), 1) k_stream(int ntiles, int nlong, Op op, StreamTrial tr) {
+template <class Op, int GW, bool LDG, int B, int DEEP>
+__global__ void __launch_bounds__(stream_threads(GW), stream_ctas_per_sm(DEEP)) k_stream(int ntiles, int nlong, Op op, StreamTrial tr) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (op.setup()) stream_run<GW, LDG, B, DEEP>(op, smem, ntiles, nlong, tr);
 }

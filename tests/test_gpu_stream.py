@@ -17,7 +17,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = ["ldg4", "ldg4deep", "ldg8b16", "cp4"]
+VARIANTS = ["ldg4", "ldg4deep", "ldg8b16", "cp4", "ldg8deep", "ldg6deep", "ldg4b16deep", "ldg4pair", "ldg6pair"]
 
 
 def sp():
