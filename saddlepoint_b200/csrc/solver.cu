@@ -721,9 +721,11 @@ void launch_sell(sp_solver *s, const SellMat &S, cudaStream_t st, const Op &op) 
 
 // Which engine runs each MID pass (-1: the tile engine, ENGINE_SELL the SELL path, else a
 // stream-engine variant). The defaults are the fastest measured on the 40M power-law LP (ms
-// per launch): the primal pass on the stream engine with 4 register-gatherer warps, 4 slots
-// in FP64 (0.255; tile engine 0.297, SELL 0.267 — 69 % of its nonzeros sit in warp rows)
-// and 4 in FP32 (0.247; SELL 0.255); the dual pass on its SELL copy in both precisions
+// per launch): the primal pass on the stream engine with 4 register-gatherer warps and 8
+// loads in flight per lane, 4 slots in FP64 (0.255; 3 slots 0.265, 6 or 8 gatherer warps
+// 0.266-0.285, 16 loads in flight 0.275-0.309, two CTAs per SM with 2 slots 0.269; tile
+// engine 0.297, SELL 0.31) and two CTAs per SM with 2 slots in FP32 (0.242; one CTA with 4
+// slots 0.246, deeper slots 0.32-0.39); the dual pass on its SELL copy in both precisions
 // (0.185 FP64, 0.182 FP32 with 512-row windows; tile engine 0.238 and 0.249, stream engine
 // 0.300 and 0.227).
 // A problem under SMALL_NNZ nonzeros keeps both passes on the tile engine: there an
@@ -739,7 +741,7 @@ int choose_engines(sp_solver *s) {
     // "large": the large-problem assignment whatever the size (tests of small LPs use it)
     const bool small = s->nnz < SMALL_NNZ && !(eng && !strcmp(eng, "large"));
     s->sv_p64 = small ? -1 : SV_LDG4_DEEP;
-    s->sv_p32 = small ? -1 : SV_LDG4;
+    s->sv_p32 = small ? -1 : SV_LDG4_PAIR;
     s->sv_d64 = small ? -1 : ENGINE_SELL;
     s->sv_d32 = small ? -1 : ENGINE_SELL;
     // test knob of the stream engine's stall path (stream.cuh: StreamTrial): the copies
