@@ -209,6 +209,10 @@ int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *param
 int sp_solver_solve(sp_solver *s, sp_solution_info *info);
 /* Resets the iterates and counters to the start of a solve (keeps ‖A'‖₂). */
 int sp_solver_reset(sp_solver *s);
+/* sp_solver_reset, then the next solve starts from (x, y) in the original problem's space
+ * (ncols and nrows entries; either may be null for zeros) as iterate and restart anchor,
+ * instead of from 0. No counterpart in the reference, whose solve always starts at 0. */
+int sp_solver_warm_start(sp_solver *s, const double *x, const double *y);
 /* Enqueues `epochs` epochs of check_every iterations without waiting; a converged
  * state turns further epochs into no-ops. */
 int sp_solver_run_epochs(sp_solver *s, uint64_t epochs);
@@ -377,9 +381,21 @@ int sp_csr_from_triplets(sp_ctx *ctx, int64_t nrows, int64_t ncols, int64_t ntri
 void sp_csr_release(sp_csr *m);
 
 /* ========================================================================
- * Part 6 — presolve. The reference's path has none; cuPDLPx, which the reference's
- * benchmark compares against, presolves (bench/README.md:1-6). Host code.
+ * Part 6 — presolve and feasibility polishing. The reference's path has neither;
+ * cuPDLPx, which the reference's benchmark compares against, has both
+ * (bench/README.md:1-6).
  * ======================================================================== */
+
+/* Feasibility polishing (as cuPDLPx applies it after a solve), on the GPU of `ctx`: from a
+ * solution (x, y) of `lp`, a warm-started FP64 solve of the feasibility problem (the same
+ * constraints, zero cost) brings x to primal feasibility within `tolerance` (relative, as the
+ * termination test measures it), and a warm-started solve of the problem with every finite
+ * bound set to zero (the same dual feasible set, zero dual objective) brings y to dual
+ * feasibility within `tolerance`. x and y are overwritten with the polished pair;
+ * `iterations` (may be null) receives the two solves' iteration counts. Each solve is capped
+ * at params->max_iterations; params may be null for the defaults. */
+int sp_polish(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *params, double tolerance, double *x, double *y,
+              uint64_t iterations[2]);
 
 typedef struct sp_presolve sp_presolve;
 

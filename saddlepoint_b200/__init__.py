@@ -32,7 +32,7 @@ __all__ = [
     "BackendError", "SolveError", "Status", "Termination", "Precision", "LpProblem", "ScaledProblem",
     "SolverParams", "Solution", "CudaBackend", "Solver", "solve", "solve_stepwise", "BatchSolver", "Server",
     "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library", "read_mps", "MpsError",
-    "csr_from_triplets", "presolve", "Presolved", "solve_presolved",
+    "csr_from_triplets", "presolve", "Presolved", "solve_presolved", "polish",
 ]
 
 
@@ -462,6 +462,14 @@ class Solver(_Handle):
     def reset(self):
         self._c(self.lib.sp_solver_reset(self.h))
 
+    def warm_start(self, x=None, y=None):
+        """Reset, then start the next solve from (x, y) in the original space (None: zeros)."""
+        xv = None if x is None else _f64(x)
+        yv = None if y is None else _f64(y)
+        if xv is not None and len(xv) != self.problem.ncols or yv is not None and len(yv) != self.problem.nrows:
+            raise ValueError("warm start vectors do not fit the problem")
+        self._c(self.lib.sp_solver_warm_start(self.h, None if xv is None else _pd(xv), None if yv is None else _pd(yv)))
+
     def run_epochs(self, epochs: int):
         self._c(self.lib.sp_solver_run_epochs(self.h, epochs))
 
@@ -678,6 +686,25 @@ def generate_transport_lp(seed: int, supplies: int = 2000, demands: int = 2000) 
     """Transportation LP: supplies × demands arcs, integer supplies/demands, costs U{1..100}."""
     g = L.GenParams(kind=2, seed=seed, supplies=supplies, demands=demands)
     return _generate(g, f"transport_{supplies}x{demands}_s{seed}")
+
+
+# ------------------------------------------------------------------ polishing
+
+def polish(problem, x, y, tolerance: float = 1e-9, params: Optional[SolverParams] = None,
+           backend: Optional[CudaBackend] = None):
+    """Feasibility polishing of a solution (x, y) of `problem` on the GPU: two warm-started FP64
+    solves bring x to primal and y to dual feasibility within `tolerance`. Returns
+    (x, y, (primal iterations, dual iterations))."""
+    b = _backend(backend)
+    p = LpProblem.from_any(problem)
+    view = _LpView(p)
+    cp = (params or SolverParams()).to_c()
+    xo, yo = _f64(x).copy(), _f64(y).copy()
+    if len(xo) != p.ncols or len(yo) != p.nrows:
+        raise ValueError("x and y do not fit the problem")
+    it = (C.c_uint64 * 2)()
+    b._check(b.lib.sp_polish(b.h, C.byref(view.s), C.byref(cp), float(tolerance), _pd(xo), _pd(yo), it), SolveError)
+    return xo, yo, (int(it[0]), int(it[1]))
 
 
 # ------------------------------------------------------------------ presolve

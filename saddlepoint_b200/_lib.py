@@ -143,6 +143,7 @@ SIGNATURES = [
     ("sp_solver_create", cint, [VP, C.POINTER(Lp), C.POINTER(Params), C.POINTER(VP)]),
     ("sp_solver_solve", cint, [VP, C.POINTER(Info)]),
     ("sp_solver_reset", cint, [VP]),
+    ("sp_solver_warm_start", cint, [VP, PD, PD]),
     ("sp_solver_run_epochs", cint, [VP, u64]),
     ("sp_solver_sync", cint, [VP]),
     ("sp_solver_info", cint, [VP, C.POINTER(Info)]),
@@ -171,6 +172,7 @@ SIGNATURES = [
     ("sp_read_mps", cint, [C.c_char_p, C.c_size_t, C.POINTER(Lp), C.POINTER(i64), C.c_char_p, C.c_size_t]),
     ("sp_csr_from_triplets", cint, [VP, i64, i64, i64, PI64, PI64, PD, C.POINTER(Csr)]),
     ("sp_csr_release", None, [C.POINTER(Csr)]),
+    ("sp_polish", cint, [VP, C.POINTER(Lp), C.POINTER(Params), dbl, PD, PD, C.POINTER(u64)]),
     ("sp_presolve_create", cint, [C.POINTER(Lp), C.POINTER(Lp), C.POINTER(VP), C.POINTER(cint)]),
     ("sp_presolve_postsolve", cint, [VP, PD, PD, PD, PD]),
     ("sp_presolve_counts", cint, [VP, PI64]),

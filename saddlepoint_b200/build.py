@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
 CU = ["backend.cu", "solver.cu", "batch.cu", "serve.cu", "noalloc.cu", "triplets.cu"]
-CPP = ["host.cpp", "mps.cpp", "presolve.cpp"]
+CPP = ["host.cpp", "mps.cpp", "presolve.cpp", "polish.cpp"]
 HEADERS = ["common.cuh", "internal.cuh", "tiles.cuh", "stream.cuh", "sell.cuh", "control.cuh", "solver_kernels.cuh", "solver_state.h", "batch_kernels.cuh"]
 
 

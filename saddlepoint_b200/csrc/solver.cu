@@ -367,6 +367,26 @@ __global__ void k_unscale(const double *xt, const double *yt, const double *cs, 
     GRID_LOOP(i, m) { y[i] = yt[i] * rs[i] / os; }
 }
 
+// A starting point given in the original space, mapped into the scaled one (the inverse of
+// k_unscale: x' = x·β / col_scale, y' = y·γ / row_scale), as iterate and anchor; the mixed
+// form's FP32 shadow of y too (the first primal pass gathers it).
+__global__ void k_warm_start(const double *x0, const double *y0, const double *cs, const double *rs,
+                             const double *scales, double *x, double *xa, double *y, double *ya, float *y32,
+                             int64_t n, int64_t m) {
+    const double bs = scales[0], os = scales[1];
+    GRID_LOOP(j, n) {
+        const double v = x0 ? x0[j] * bs / cs[j] : 0.0;
+        x[j] = v;
+        xa[j] = v;
+    }
+    GRID_LOOP(i, m) {
+        const double v = y0 ? y0[i] * os / rs[i] : 0.0;
+        y[i] = v;
+        ya[i] = v;
+        if (y32) y32[i] = (float)v;
+    }
+}
+
 }  // namespace sp
 
 // ============================================================ host side
@@ -1274,6 +1294,30 @@ extern "C" int sp_solver_reset(sp_solver *s) {
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     s->launched = 0;
     s->time_limited = false;
+    return SP_OK;
+}
+
+extern "C" int sp_solver_warm_start(sp_solver *s, const double *x, const double *y) {
+    if (!s) return SP_ERR_INVALID;
+    int rc = sp_solver_reset(s);
+    if (rc) return rc;
+    if (!x && !y) return SP_OK;
+    cudaStream_t st = s->ctx->stream;
+    double *dx = nullptr, *dy = nullptr;
+    if (x && (rc = dalloc(&dx, s->n))) return rc;
+    if (y && (rc = dalloc(&dy, s->m))) {
+        dfree(dx, st);
+        return rc;
+    }
+    if (x && s->n) SP_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * s->n, cudaMemcpyHostToDevice, st));
+    if (y && s->m) SP_CUDA_TRY(cudaMemcpyAsync(dy, y, sizeof(double) * s->m, cudaMemcpyHostToDevice, st));
+    k_warm_start<<<grid_of(s->ctx, std::max(s->n, s->m)), NT, 0, st>>>(dx, dy, s->col_scale, s->row_scale, s->scales,
+                                                                        s->x, s->xa, s->y, s->ya, s->mixed ? s->y32 : nullptr,
+                                                                        s->n, s->m);
+    SP_CUDA_TRY(cudaGetLastError());
+    SP_CUDA_TRY(cudaStreamSynchronize(st));
+    dfree(dx, st);
+    dfree(dy, st);
     return SP_OK;
 }
 
