@@ -118,6 +118,17 @@ class Clocks:
             self.proc = None
         return self
 
+    def settle(self, timeout_s: float = 3.0):
+        """Waits until the sampler has written its first line (or `timeout_s`), so that
+        starting nvidia-smi does not overlap the work it is sampling."""
+        import select
+
+        if not self.proc or not self.proc.stdout:
+            return
+        r, _, _ = select.select([self.proc.stdout], [], [], timeout_s)
+        if r:
+            self.proc.stdout.readline()  # a sample taken before the timed work: not kept
+
     def __exit__(self, *a):
         self.lines = []
         if self.proc:
@@ -266,10 +277,11 @@ def time_form(sp, torch, lp, backend, precision, steps, warmup, dist, device):
     stream = torch.cuda.ExternalStream(backend.stream(), device=f"cuda:{device}")
     solver.run_epochs(warmup)
     solver.sync()
-    dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(device)
     with Clocks(device) as clk:
+        clk.settle()  # the sampler's start-up stays out of the timed region
+        dist.barrier()
+        torch.cuda.synchronize(device)
         e0.record(stream)
         solver.run_epochs(steps)
         e1.record(stream)
@@ -557,8 +569,9 @@ def batch_forms(sp, backend, dist, lps, runs, warm=True):
         if warm:
             b.solve()
         times = []
-        dist.barrier()
         with Clocks(dist.local) as clk:
+            clk.settle()
+            dist.barrier()
             for _ in range(runs):
                 res, t = b.solve()
                 times.append(t)
