@@ -33,7 +33,7 @@ struct sp_batch {
     int *d_counter = nullptr;
     double *av0 = nullptr, *tv0 = nullptr;  // the original values (the kernel scales in place)
     size_t smem = 0;
-    double tuned_us[2][8] = {};  // per-iteration µs of each variant at the calibration sizes
+    double tuned_us[4][8] = {};  // per-iteration µs of each tuned shape at the calibration sizes
     int tuned_nnz[8] = {};
     int tuned_points = 0;
     sp_solver_params params{};  // every instance's parameters (the hand-off solves use them too)
@@ -42,12 +42,26 @@ struct sp_batch {
 namespace sp {
 
 // Lanes per row for a matrix whose rows hold `mean` entries on average: the
-// smallest power of two that leaves each lane about three products (one lane per
+// smallest power of two that leaves each lane about `per_lane` products (one lane per
 // row keeps the reference's summation order for short rows).
-int lanes_for(double mean) {
+int lanes_for(double mean, int per_lane = 3) {
     int L = 1;
-    while (L < 32 && L * 3 < mean) L <<= 1;
+    while (L < 32 && L * per_lane < mean) L <<= 1;
     return L;
+}
+
+// The shapes the tuner times: lane groups with about 3, 2 or 6 products per lane, and the
+// staged tiles.
+constexpr int TUNE_SHAPES = 4;
+constexpr int SHAPE_TILES = 1;
+int shape_per_lane(int shape) { return shape == 2 ? 2 : shape == 3 ? 6 : 3; }
+
+// Gives instance I the SpMV shape `shape` (its variant and lanes per row).
+void apply_shape(BatchInst &I, int shape) {
+    I.variant = shape == SHAPE_TILES ? VARIANT_TILES : VARIANT_LANES;
+    const int k = shape_per_lane(shape);
+    I.lanes_a = lanes_for(I.m ? (double)I.nnz / I.m : 0.0, k);
+    I.lanes_t = lanes_for(I.n ? (double)I.nnz / I.n : 0.0, k);
 }
 
 template <class T>
@@ -57,20 +71,21 @@ int balloc(sp_batch *b, T **p, int64_t n) {
     return SP_OK;
 }
 
-// The autotuner. Once per device it times the two SpMV variants — lane groups
-// (rows dealt to L lanes that walk them with strided loads) and staged tiles (the
-// single-LP tile passes) — on built-in seeded reference LPs that span the sizes of
-// the batched workload, each alone in one CTA, as the difference of a 320- and a
-// 64-iteration run (the scaling passes and the power iteration cancel). Every
-// instance then gets the variant whose interpolated per-iteration time at its size
-// (log nnz) is lower. The choice depends on the instance alone, never on the rest
+// The autotuner. Once per device it times four SpMV shapes — lane groups (rows dealt to
+// L lanes that walk them with strided loads, L the smallest power of two leaving each
+// lane about 3, 2 or 6 products) and staged tiles (the single-LP tile passes) — on
+// built-in seeded reference LPs that span the sizes of the batched workload, each alone
+// in one CTA, as the difference of a 320- and a 64-iteration run (the scaling passes and
+// the power iteration cancel). Every instance then gets the shape whose interpolated
+// per-iteration time at its size (log nnz) is lowest, with its own L from its mean row
+// lengths. The choice depends on the instance alone, never on the rest
 // of the batch, so an instance is computed the same way alone and in any mix.
 // SP_BATCH_VARIANT=lanes|tiles in the environment forces one variant.
 struct TuneTable {
     bool ready = false;
     int npts = 0;
     int nnz[8] = {};
-    double us[2][8] = {};
+    double us[TUNE_SHAPES][8] = {};
 };
 static TuneTable g_tune[64];
 static std::mutex g_tune_mu;
@@ -128,8 +143,8 @@ int calibrate(sp_ctx *ctx, TuneTable *T) {
             return SP_OK;
         };
         const int npts = (int)inst.size();
-        for (int v = 0; v < 2 && !rc; ++v) {
-            for (auto &I : inst) I.variant = v;
+        for (int v = 0; v < TUNE_SHAPES && !rc; ++v) {
+            for (auto &I : inst) apply_shape(I, v);
             rc = cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInst) * npts, cudaMemcpyHostToDevice) == cudaSuccess
                      ? SP_OK
                      : SP_ERR_CUDA;
@@ -166,8 +181,7 @@ int tune_variants(sp_batch *b) {
         b->tuned_points = T.npts;
         for (int p = 0; p < T.npts; ++p) {
             b->tuned_nnz[p] = T.nnz[p];
-            b->tuned_us[0][p] = T.us[0][p];
-            b->tuned_us[1][p] = T.us[1][p];
+            for (int v = 0; v < TUNE_SHAPES; ++v) b->tuned_us[v][p] = T.us[v][p];
         }
         auto estimate = [&](int v, int nnz) {
             const double x = std::log(std::max(1, nnz));
@@ -178,11 +192,14 @@ int tune_variants(sp_batch *b) {
             const double f = x1 > x0 ? std::min(1.0, std::max(0.0, (x - x0) / (x1 - x0))) : 0.0;
             return T.us[v][p] + f * (T.us[v][p + 1] - T.us[v][p]);
         };
-        for (auto &I : inst)
-            I.variant =
-                estimate(VARIANT_TILES, I.nnz) <= estimate(VARIANT_LANES, I.nnz) ? VARIANT_TILES : VARIANT_LANES;
+        for (auto &I : inst) {
+            int best = 0;
+            for (int v = 1; v < TUNE_SHAPES; ++v)
+                if (estimate(v, I.nnz) < estimate(best, I.nnz)) best = v;
+            apply_shape(I, best);
+        }
     } else {
-        for (auto &I : inst) I.variant = forced;
+        for (auto &I : inst) apply_shape(I, forced == VARIANT_TILES ? SHAPE_TILES : 0);
     }
     cudaStream_t st = b->ctx->stream;
     SP_CUDA_TRY(cudaMemcpyAsync(b->d_inst, inst.data(), sizeof(BatchInst) * b->count, cudaMemcpyHostToDevice, st));
@@ -367,8 +384,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
         I.m = (int)A.nrows;
         I.n = (int)A.ncols;
         I.nnz = (int)A.nnz;
-        I.lanes_a = lanes_for(A.nrows ? (double)A.nnz / A.nrows : 0.0);
-        I.lanes_t = lanes_for(A.ncols ? (double)A.nnz / A.ncols : 0.0);
+        apply_shape(I, 0);
         I.rpa = rpa;
         I.rpt = rpt;
         I.nz = nz;
