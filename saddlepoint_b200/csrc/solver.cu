@@ -1328,6 +1328,16 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
         return fail(SP_ERR_INVALID, "sp_solver_create: null argument");
     if ((rc = validate_lp(lp))) return rc;
     double t0 = now_s();
+    // SP_SETUP_TRACE=1: each set-up stage's wall time on stderr (the stages synchronise)
+    const bool trace = getenv("SP_SETUP_TRACE") != nullptr;
+    double tl = t0;
+    auto stage = [&](const char *what) {
+        if (!trace) return;
+        cudaStreamSynchronize(ctx->stream);
+        const double t = now_s();
+        fprintf(stderr, "setup %-12s %8.2f ms\n", what, (t - tl) * 1e3);
+        tl = t;
+    };
     auto *s = new sp_solver();
     s->ctx = ctx;
     sp_solver_params_default(&s->prm);
@@ -1347,13 +1357,16 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
         return code;
     };
     if ((rc = upload_csr(ctx, &lp->a, &s->A, false))) return cleanup(rc);
+    stage("upload");
     if ((rc = transpose_on_device(s))) return cleanup(rc);
+    stage("transpose");
     if ((rc = dalloc(&s->c, n)) || (rc = dalloc(&s->lc, m)) || (rc = dalloc(&s->uc, m)) || (rc = dalloc(&s->lv, n)) ||
         (rc = dalloc(&s->uv, n)) || (rc = dalloc(&s->pf, m)) || (rc = dalloc(&s->df, n)) ||
         (rc = dalloc(&s->row_scale, m)) || (rc = dalloc(&s->col_scale, n)) || (rc = dalloc(&s->scales, 2)) ||
         (rc = dalloc(&s->norms, 4)))
         return cleanup(rc);
     if ((rc = scale_on_device(s, lp))) return cleanup(rc);
+    stage("scaling");
     double hn[4], hs[2];
     SP_CUDA_TRY(cudaMemcpyAsync(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost, ctx->stream));
     SP_CUDA_TRY(cudaMemcpyAsync(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1384,9 +1397,12 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     SP_CUDA_TRY(cudaMallocHost(&s->h_st, sizeof(DevState) * (SolverLookahead + 2)));
     if ((rc = set_smem_limits())) return cleanup(rc);
     if ((rc = choose_engines(s))) return cleanup(rc);
+    stage("engines");
     // ‖A'‖₂ and η (solver.rs:316)
     if ((rc = sp_solver_reset(s))) return cleanup(rc);
+    stage("buffers");
     if ((rc = power_iteration(s))) return cleanup(rc);
+    stage("power");
     DevParams dp{};
     const sp_solver_params &P = s->prm;
     dp.tolerance = P.tolerance;
