@@ -250,12 +250,15 @@ __global__ void k_scale_vectors(const double *c, const double *lc, const double 
 // the loads, sets the pace). Block b computes norm b: the bound and cost norms of
 // the original problem (norms[2], norms[3]) and of the scaled one (norms[0],
 // norms[1]).
-constexpr int SEQ_CHUNK = 1024;
+constexpr int SEQ_CHUNK = 2048;
 
 __global__ void __launch_bounds__(NT) k_seq_norms(const double *olc, const double *ouc, const double *oc,
                                                   const double *lc, const double *uc, const double *c, int64_t m,
                                                   int64_t n, double *norms) {
-    __shared__ double sa[2][SEQ_CHUNK], sb[2][SEQ_CHUNK];
+    // The terms of the sum are independent of one another: threads 1..NT-1 form the next
+    // chunk's terms (each with the reference's operations) while thread 0 adds this chunk's
+    // in index order; the additions, the one dependent chain, are exactly the reference's.
+    __shared__ double st[2][SEQ_CHUNK];
     const int which = blockIdx.x & 1;  // 0: bound norm over m rows, 1: cost norm over n columns
     const bool orig = blockIdx.x < 2;
     const double *a = which == 0 ? (orig ? olc : lc) : (orig ? oc : c);
@@ -266,9 +269,13 @@ __global__ void __launch_bounds__(NT) k_seq_norms(const double *olc, const doubl
         const int64_t base = k * SEQ_CHUNK;
         for (int i = threadIdx.x - 1; i < SEQ_CHUNK; i += NT - 1) {
             const int64_t e = base + i;
-            if (e < len) {
-                sa[buf][i] = a[e];
-                if (which == 0) sb[buf][i] = b[e];
+            if (e >= len) break;
+            if (which == 0) {  // finite_bound_norm's term (scaling.rs:191-201)
+                const double l = isfinite(a[e]) ? a[e] : 0.0;
+                const double u = isfinite(b[e]) ? b[e] : 0.0;
+                st[buf][i] = (l == u) ? l * l : l * l + u * u;
+            } else {
+                st[buf][i] = a[e] * a[e];  // norm2's term (scaling.rs:186-188)
             }
         }
     };
@@ -279,15 +286,16 @@ __global__ void __launch_bounds__(NT) k_seq_norms(const double *olc, const doubl
         const int buf = (int)(k & 1);
         if (threadIdx.x == 0) {
             const int cnt = (int)min((int64_t)SEQ_CHUNK, len - k * SEQ_CHUNK);
-            if (which == 0) {
-                for (int i = 0; i < cnt; ++i) {
-                    const double l = isfinite(sa[buf][i]) ? sa[buf][i] : 0.0;
-                    const double u = isfinite(sb[buf][i]) ? sb[buf][i] : 0.0;
-                    s += (l == u) ? l * l : l * l + u * u;
-                }
-            } else {
-                for (int i = 0; i < cnt; ++i) s += sa[buf][i] * sa[buf][i];
+            const double *t = st[buf];
+            int i = 0;
+            for (; i + 8 <= cnt; i += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = t[i + u];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) s += v[u];
             }
+            for (; i < cnt; ++i) s += t[i];
         } else if (k + 1 < nchunks) {
             stage(k + 1, buf ^ 1);
         }
