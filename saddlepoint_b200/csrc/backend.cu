@@ -258,6 +258,8 @@ extern "C" int sp_ctx_create(int ordinal, sp_ctx **out) {
     ctx->cc_major = prop.major;
     ctx->cc_minor = prop.minor;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->aux_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaMalloc(&ctx->d_partials, sizeof(double) * RED_BLOCKS * RED_SLOTS * 4) != cudaSuccess ||
         cudaMalloc(&ctx->d_result, sizeof(double) * RED_SLOTS * 4) != cudaSuccess ||
         cudaMallocHost(&ctx->h_result, sizeof(double) * RED_SLOTS * 4) != cudaSuccess ||
@@ -275,11 +277,14 @@ extern "C" void sp_ctx_destroy(sp_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->aux) cudaStreamSynchronize(ctx->aux);
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_result);
     cudaFreeHost(ctx->h_result);
     cudaFree(ctx->d_tiles);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->aux) cudaStreamDestroy(ctx->aux);
+    if (ctx->aux_ev) cudaEventDestroy(ctx->aux_ev);
     if (t_ctx_is(ctx)) set_current_ctx(nullptr);
     delete ctx;
 }
@@ -415,30 +420,37 @@ int upload_csr(sp_ctx *ctx, const sp_csr *h, DevCsr *d, bool want_f32) {
         if (i > 0 && h->row_ptr[i] < h->row_ptr[i - 1]) return fail(SP_ERR_INVALID, "CSR row_ptr not monotone");
         rp32[i] = (int)h->row_ptr[i];
     }
-    std::vector<Tile> tiles = build_tiles(h->row_ptr, h->nrows);
-    d->ntiles = (int)tiles.size();
-    d->nlong = count_long_tiles(tiles);
     size_t nz = (size_t)std::max<int64_t>(h->nnz, 1) + CSR_PAD;
     int rc;
     if ((rc = dmalloc((void **)&d->rp, sizeof(int) * (h->nrows + 1 + CSR_PAD))) ||
-        (rc = dmalloc((void **)&d->ci, sizeof(int) * nz)) || (rc = dmalloc((void **)&d->v, sizeof(double) * nz)) ||
-        (rc = dmalloc((void **)&d->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1))))
+        (rc = dmalloc((void **)&d->ci, sizeof(int) * nz)) || (rc = dmalloc((void **)&d->v, sizeof(double) * nz)))
         return rc;
+    // the copies first: from page-locked memory they run while the host builds the tile plan
     SP_CUDA_TRY(cudaMemcpyAsync(d->rp, rp32.data(), sizeof(int) * (h->nrows + 1), cudaMemcpyHostToDevice, ctx->stream));
     if (h->nnz) {
         SP_CUDA_TRY(cudaMemcpyAsync(d->ci, h->col_idx, sizeof(int) * h->nnz, cudaMemcpyHostToDevice, ctx->stream));
         SP_CUDA_TRY(cudaMemcpyAsync(d->v, h->values, sizeof(double) * h->nnz, cudaMemcpyHostToDevice, ctx->stream));
     }
+    // an early return waits for the copies, which read the caller's memory and rp32
+    auto bail = [&](int code) {
+        cudaStreamSynchronize(ctx->stream);
+        return code;
+    };
+    std::vector<Tile> tiles = build_tiles(h->row_ptr, h->nrows);
+    d->ntiles = (int)tiles.size();
+    d->nlong = count_long_tiles(tiles);
+    if ((rc = dmalloc((void **)&d->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)))) return bail(rc);
     if (!tiles.empty())
         SP_CUDA_TRY(cudaMemcpyAsync(d->tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice,
                                     ctx->stream));
     const std::vector<uint16_t> sched = build_schedule(h->row_ptr, h->nrows, tiles);
-    if ((rc = dmalloc((void **)&d->sched, sizeof(uint16_t) * (std::max<int64_t>(h->nrows, 1) + CSR_PAD)))) return rc;
+    if ((rc = dmalloc((void **)&d->sched, sizeof(uint16_t) * (std::max<int64_t>(h->nrows, 1) + CSR_PAD))))
+        return bail(rc);
     if (h->nrows)
         SP_CUDA_TRY(cudaMemcpyAsync(d->sched, sched.data(), sizeof(uint16_t) * h->nrows, cudaMemcpyHostToDevice,
                                     ctx->stream));
     if (want_f32) {
-        if ((rc = dmalloc((void **)&d->v32, sizeof(float) * nz))) return rc;
+        if ((rc = dmalloc((void **)&d->v32, sizeof(float) * nz))) return bail(rc);
     }
     // the host vectors die with this call
     SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));

@@ -13,6 +13,8 @@ struct sp_ctx {
     std::string name;
     std::string last_error;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;     // a second stream for set-up work beside `stream`'s
+    cudaEvent_t aux_ev = nullptr;   // orders `aux` after work on `stream`
     double *d_partials = nullptr;  // stage-one partials of the trait-method reductions
     double *d_result = nullptr;    // their final values
     double *h_result = nullptr;    // pinned copy read by the host

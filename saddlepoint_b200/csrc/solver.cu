@@ -100,14 +100,24 @@ __global__ void k_halpern_x0(SolverPtrs s, int64_t n) {
 
 // ============================================================ power iteration
 
-__global__ void k_power_init(double *v, int64_t n, double *part) {
-    // start = 1 + 0.01 (j mod 7) (solver.rs:221); one block reduces ‖start‖² in order.
+// start = 1 + 0.01 (j mod 7) (solver.rs:221)
+__device__ __forceinline__ double power_start(int64_t j) { return 1.0 + 0.01 * (double)(j % 7); }
+
+__global__ void k_power_fill(double *v, int64_t n) {
+    GRID_LOOP(j, n) { v[j] = power_start(j); }
+}
+
+// ‖start‖², reduced by one block in a fixed order (the terms are formed, not loaded;
+// j mod 7 steps by NT mod 7 from one term of a thread to its next).
+__global__ void k_power_init(int64_t n, double *part) {
     __shared__ double sh[NT / 32];
     double s[1] = {0.0};
+    int r = threadIdx.x % 7;
     for (int64_t j = threadIdx.x; j < n; j += NT) {
-        const double x = 1.0 + 0.01 * (double)(j % 7);
-        v[j] = x;
+        const double x = 1.0 + 0.01 * (double)r;
         s[0] += x * x;
+        r += NT % 7;
+        if (r >= 7) r -= 7;
     }
     block_sum<1>(s, sh);
     if (threadIdx.x == 0) part[0] = s[0];
@@ -202,27 +212,199 @@ __global__ void k_row_pc(const int *rp, const double *v, int64_t rows, double al
     }
 }
 
-// values[k] *= r[i] * c[j] for every entry (i, j) (CsrMatrix::scale, problem.rs:120-126),
-// applied to A' (rows i) and, in the same pass over its own layout, to A'ᵀ.
+// The scaling's sweeps. The reference scales A' in place with a.scale(r, c)
+// (values[k] *= r[i] * c[j], problem.rs:118-125) and forms each next factor from the
+// scaled values (scaling.rs:53-79); it builds A'ᵀ only at the end. Here A'ᵀ exists
+// from the start, so every step updates both layouts with the same operations (an
+// entry gets the same roundings in both) and forms the statistic of the next step from
+// the values it has just written, in the same sweep: one read and one write of each
+// layout per step, instead of a statistics sweep plus an apply sweep of both layouts
+// per half-step, and no multiplications by the all-ones vector (r·1 = r exactly).
+enum NextStat : int { NEXT_NONE = 0, NEXT_GEO = 1, NEXT_MAX = 2 };
+
 template <int G>
-__global__ void k_apply_rows(const int *rp, const int *ci, double *v, int64_t rows, const double *r, const double *c,
-                             int transposed) {
-    const int lane = threadIdx.x & 31, sub = lane % G;
-    const int64_t grp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) / G;
-    for (int64_t i = grp; i < rows; i += ng) {
-        for (int k = rp[i] + sub; k < rp[i + 1]; k += G) {
-            const int j = ci[k];
-            // A'ᵀ row i is column i of A': the factor is still r[row] * c[col].
-            const double f = transposed ? r[j] * c[i] : r[i] * c[j];
-            v[k] *= f;
+__device__ __forceinline__ void group_min_max(double &lo, double &hi) {
+    for (int o = G / 2; o; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+}
+
+// The factor a NEXT statistic gives a row: 1/sqrt(min·max) of its magnitudes
+// (min_max, scaling.rs:159-178: an empty or all-zero row counts min as 0), or
+// 1/sqrt(max) (the Ruiz step, scaling.rs:68-70).
+template <int NEXT>
+__device__ __forceinline__ double next_factor(double lo, double hi) {
+    return NEXT == NEXT_GEO ? inv_sqrt_d((hi == 0.0 ? 0.0 : lo) * hi) : inv_sqrt_d(hi);
+}
+
+// Short rows (at most SWEEP_TRIPS·G entries) go to a group of G lanes; a longer row is
+// taken by the whole warp after the group pass (a ballot finds them), so one long row does
+// not hold up the warp's other groups for many trips. Neither choice changes a bit: every
+// entry is computed alone and min / max do not depend on the order. (Measured on the 40M
+// LP's layouts: plain loads beat chunks of loads issued ahead and the streaming cache hints
+// here, 0.31 against 0.42-0.69 ms on A', 0.37 against 0.52 ms on A'ᵀ.)
+constexpr int SWEEP_TRIPS = 4;
+
+// Entry k's new value: GEO2 (v·own)·gat, else v·(own·gat).
+template <bool GEO2>
+__device__ __forceinline__ double sweep_value(double v, double own, double g) {
+    return GEO2 ? (v * own) * g : v * (own * g);
+}
+
+// Entries k, k + step, ... < k1 of one row (a long row: step 32, all lanes): new values
+// written, min / max of their magnitudes into lo / hi.
+template <bool GEO2, bool STATS>
+__device__ __forceinline__ void sweep_span(const int *__restrict__ ci, double *__restrict__ v,
+                                           const double *__restrict__ gat, int k, int k1, int step, double f,
+                                           double &lo, double &hi) {
+    for (; k < k1; k += step) {
+        const double a = sweep_value<GEO2>(v[k], f, __ldg(gat + ci[k]));
+        v[k] = a;
+        if (STATS) {
+            lo = fmin(lo, fabs(a));
+            hi = fmax(hi, fabs(a));
         }
     }
 }
 
-__global__ void k_mul_inplace(double *s, const double *f, int64_t n) {
-    GRID_LOOP(i, n) { s[i] *= f[i]; }
+// One sweep over a layout, G lanes per row: every entry of row `r` is multiplied by its
+// row's factor own[r] and the factor gat[ci] of its other index, as
+//   GEO2:  (v·own)·gat — the A' side of a geometric-mean pass, whose two applies each
+//          had a factor of 1 on the other side (two roundings, as the reference);
+//   else:  v·(own·gat) — Ruiz and Pock-Chambolle, one product as problem.rs:123 forms
+//          it (on the A'ᵀ side the product is c_j·r_i, the same number: IEEE
+//          multiplication commutes).
+// scale[r] *= own[r] (apply, scaling.rs:181-183); next[r] = the NEXT statistic's
+// factor of the row's new values.
+template <int G, bool GEO2, int NEXT>
+__global__ void __launch_bounds__(NT) k_scale_sweep(const int *__restrict__ rp, const int *__restrict__ ci,
+                                                    double *__restrict__ v, int64_t rows,
+                                                    const double *__restrict__ own, const double *__restrict__ gat,
+                                                    double *__restrict__ scale, double *__restrict__ next) {
+    constexpr bool STATS = NEXT != NEXT_NONE;
+    const int lane = threadIdx.x & 31, sub = lane % G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * (32 / G); base < rows; base += nw * (32 / G)) {
+        const int64_t r = base + lane / G;
+        const bool live = r < rows;
+        const int k0 = live ? rp[r] : 0, k1 = live ? rp[r + 1] : 0;
+        const bool longrow = k1 - k0 > SWEEP_TRIPS * G;
+        const double f = live ? own[r] : 1.0;
+        double lo = INFINITY, hi = 0.0;
+        if (!longrow) sweep_span<GEO2, STATS>(ci, v, gat, k0 + sub, k1, G, f, lo, hi);
+        if (STATS) group_min_max<G>(lo, hi);
+        if (sub == 0 && live && !longrow) {
+            scale[r] *= f;
+            if (STATS) next[r] = next_factor<NEXT>(lo, hi);
+        }
+        for (unsigned mask = __ballot_sync(0xffffffffu, sub == 0 && longrow); mask; mask &= mask - 1) {
+            const int src = __ffs(mask) - 1;
+            const int a = __shfl_sync(0xffffffffu, k0, src), b = __shfl_sync(0xffffffffu, k1, src);
+            const double ff = __shfl_sync(0xffffffffu, f, src);
+            double l2 = INFINITY, h2 = 0.0;
+            sweep_span<GEO2, STATS>(ci, v, gat, a + lane, b, 32, ff, l2, h2);
+            if (STATS) group_min_max<32>(l2, h2);
+            if (lane == 0) {
+                const int64_t rr = base + src / G;
+                scale[rr] *= ff;
+                if (STATS) next[rr] = next_factor<NEXT>(l2, h2);
+            }
+        }
+    }
 }
+
+// The A'ᵀ side of a geometric-mean pass (row j of A'ᵀ is column j of A'): the row factor
+// of A' (gathered) comes first; the column factor c_j = 1/sqrt(min·max) of the column
+// after it (scaling.rs:64-65) needs the whole column, so a first walk forms it from the
+// products v·r and a second writes (v·r)·c_j — from the products a short row's lanes
+// kept in registers, a long row's formed again. fac[j] = c_j (the A' side gathers it),
+// scale[j] *= c_j; NEXT_MAX also gives the first Ruiz factor of the column from the
+// written values.
+template <int G, int NEXT>
+__global__ void __launch_bounds__(NT) k_scale_geo_cols(const int *__restrict__ rp, const int *__restrict__ ci,
+                                                       double *__restrict__ v, int64_t rows,
+                                                       const double *__restrict__ gat, double *__restrict__ fac,
+                                                       double *__restrict__ scale, double *__restrict__ next) {
+    constexpr bool STATS = NEXT != NEXT_NONE;
+    const int lane = threadIdx.x & 31, sub = lane % G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * (32 / G); base < rows; base += nw * (32 / G)) {
+        const int64_t r = base + lane / G;
+        const bool live = r < rows;
+        const int k0 = live ? rp[r] : 0, k1 = live ? rp[r + 1] : 0;
+        const bool longrow = k1 - k0 > SWEEP_TRIPS * G;
+        double pr[SWEEP_TRIPS];
+        double lo = INFINITY, hi = 0.0;
+        if (!longrow) {
+            int c[SWEEP_TRIPS];
+            double x[SWEEP_TRIPS];
+#pragma unroll
+            for (int t = 0; t < SWEEP_TRIPS; ++t) {
+                const int k = k0 + sub + t * G;
+                if (k < k1) {
+                    c[t] = __ldcs(ci + k);
+                    x[t] = __ldcs(v + k);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < SWEEP_TRIPS; ++t)
+                if (k0 + sub + t * G < k1) {
+                    pr[t] = x[t] * __ldg(gat + c[t]);
+                    lo = fmin(lo, fabs(pr[t]));
+                    hi = fmax(hi, fabs(pr[t]));
+                }
+        }
+        group_min_max<G>(lo, hi);
+        const double cf = next_factor<NEXT_GEO>(lo, hi);
+        double lo2 = INFINITY, hi2 = 0.0;
+        if (!longrow) {
+#pragma unroll
+            for (int t = 0; t < SWEEP_TRIPS; ++t) {
+                const int k = k0 + sub + t * G;
+                if (k < k1) {
+                    const double a = pr[t] * cf;
+                    __stcs(v + k, a);
+                    if (STATS) hi2 = fmax(hi2, fabs(a));
+                }
+            }
+        }
+        if (STATS) group_min_max<G>(lo2, hi2);
+        if (sub == 0 && live && !longrow) {
+            fac[r] = cf;
+            scale[r] *= cf;
+            if (STATS) next[r] = next_factor<NEXT>(lo2, hi2);
+        }
+        for (unsigned mask = __ballot_sync(0xffffffffu, sub == 0 && longrow); mask; mask &= mask - 1) {
+            const int src = __ffs(mask) - 1;
+            const int a = __shfl_sync(0xffffffffu, k0, src), b = __shfl_sync(0xffffffffu, k1, src);
+            double l3 = INFINITY, h3 = 0.0;
+            for (int k = a + lane; k < b; k += 32) {
+                const double p = fabs(v[k] * __ldg(gat + ci[k]));  // read again below: cached loads
+                l3 = fmin(l3, p);
+                h3 = fmax(h3, p);
+            }
+            group_min_max<32>(l3, h3);
+            const double c3 = next_factor<NEXT_GEO>(l3, h3);
+            double l4 = INFINITY, h4 = 0.0;
+            for (int k = a + lane; k < b; k += 32) {
+                const double x = (v[k] * __ldg(gat + ci[k])) * c3;
+                v[k] = x;
+                if (STATS) h4 = fmax(h4, fabs(x));
+            }
+            if (STATS) group_min_max<32>(l4, h4);
+            if (lane == 0) {
+                const int64_t rr = base + src / G;
+                fac[rr] = c3;
+                scale[rr] *= c3;
+                if (STATS) next[rr] = next_factor<NEXT>(l4, h4);
+            }
+        }
+    }
+}
+
 __global__ void k_fill(double *v, double x, int64_t n) {
     GRID_LOOP(i, n) { v[i] = x; }
 }
@@ -1047,86 +1229,198 @@ void solver_release(sp_solver *s) {
 
 // Scaling passes on the device (ScaledProblem::new, scaling.rs:53-103). A' and
 // A'ᵀ are kept in step: each pass multiplies both by the same r_i * c_j products.
-int scale_on_device(sp_solver *s, const sp_lp *lp) {
+// The norms of the bounds and costs (k_seq_norms, sequential sums: tens of ms on a
+// large problem) and the rescaling that depends on them run on the context's second
+// stream, beside the power iteration, which needs only the scaled matrix. SideNorms
+// holds that work until join(): the host waits for the second stream, and the main
+// stream then releases the original vectors the side work read.
+struct SideNorms {
+    sp_solver *s = nullptr;
+    double *keep[3] = {};
+    void arm(sp_solver *solver, double *a, double *b, double *c) {
+        s = solver;
+        keep[0] = a;
+        keep[1] = b;
+        keep[2] = c;
+    }
+    cudaError_t join() {
+        if (!s) return cudaSuccess;
+        const cudaError_t e = cudaStreamSynchronize(s->ctx->aux);
+        for (double *&b : keep) {
+            dfree(b, s->ctx->stream);
+            b = nullptr;
+        }
+        s = nullptr;
+        return e;
+    }
+    ~SideNorms() { join(); }
+};
+
+// Calls f(std::integral_constant<int, G>) for the group size g (2, 4, 8, 16 or 32).
+template <class F>
+void with_group(int g, F &&f) {
+    switch (g) {
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 32>{}); break;
+    }
+}
+
+template <int G>
+void launch_sweep(const DevCsr &M, bool geo2, int next, int grid, cudaStream_t st, const double *own,
+                  const double *gat, double *scale, double *nxt) {
+#define SP_SWEEP(GEO, NX) k_scale_sweep<G, GEO, NX><<<grid, NT, 0, st>>>(M.rp, M.ci, M.v, M.nrows, own, gat, scale, nxt)
+    if (geo2) {
+        if (next == NEXT_GEO) SP_SWEEP(true, NEXT_GEO);
+        else if (next == NEXT_MAX) SP_SWEEP(true, NEXT_MAX);
+        else SP_SWEEP(true, NEXT_NONE);
+    } else {
+        if (next == NEXT_MAX) SP_SWEEP(false, NEXT_MAX);
+        else SP_SWEEP(false, NEXT_NONE);
+    }
+#undef SP_SWEEP
+}
+
+int scale_on_device(sp_solver *s, const sp_lp *lp, const std::vector<int> &rp_t, SideNorms *side) {
     sp_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int64_t m = s->m, n = s->n, nnz = s->nnz;
     const sp_solver_params &P = s->prm;
-    double *r, *c, *ones_m, *ones_n;
+    double *rb[2] = {}, *cb[2] = {};  // factors of the rows of A' and of its columns (two of each)
     int rc;
-    if ((rc = dalloc(&r, m)) || (rc = dalloc(&c, n)) || (rc = dalloc(&ones_m, m)) || (rc = dalloc(&ones_n, n))) return rc;
-    const int gm = grid_of(ctx, m), gn = grid_of(ctx, n);
-    // lanes per row of the row passes: about half the mean row length, 4 to 32
-    auto group_of = [](int64_t z, int64_t rows) {
-        const int64_t half = rows > 0 ? (z / rows + 1) / 2 : 1;
-        int g = 4;
-        while (g < 32 && g < half) g *= 2;
-        return g;
-    };
-    const int Gm = group_of(nnz, m), Gn = group_of(nnz, n);
-    const int wm = grid_of(ctx, m * Gm), wn = grid_of(ctx, n * Gn);
-    // K<G><<<...>>>(args) for the group size g
-#define SP_ROW_LAUNCH(K, g, grid, ...)                                     \
-    do {                                                                  \
-        switch (g) {                                                      \
-        case 4: K<4><<<grid, NT, 0, st>>>(__VA_ARGS__); break;            \
-        case 8: K<8><<<grid, NT, 0, st>>>(__VA_ARGS__); break;            \
-        case 16: K<16><<<grid, NT, 0, st>>>(__VA_ARGS__); break;          \
-        default: K<32><<<grid, NT, 0, st>>>(__VA_ARGS__); break;          \
-        }                                                                 \
-    } while (0)
-    k_fill<<<gm, NT, 0, st>>>(ones_m, 1.0, m);
-    k_fill<<<gn, NT, 0, st>>>(ones_n, 1.0, n);
-    k_fill<<<gm, NT, 0, st>>>(s->row_scale, 1.0, m);
-    k_fill<<<gn, NT, 0, st>>>(s->col_scale, 1.0, n);
-    auto apply = [&](const double *rr, const double *cc) {  // apply (scaling.rs:180-184)
-        if (nnz) {
-            SP_ROW_LAUNCH(k_apply_rows, Gm, wm, s->A.rp, s->A.ci, s->A.v, m, rr, cc, 0);
-            SP_ROW_LAUNCH(k_apply_rows, Gn, wn, s->AT.rp, s->AT.ci, s->AT.v, n, rr, cc, 1);
-        }
-        k_mul_inplace<<<gm, NT, 0, st>>>(s->row_scale, rr, m);
-        k_mul_inplace<<<gn, NT, 0, st>>>(s->col_scale, cc, n);
-    };
-    for (uint64_t pass = 0; pass < P.geometric_mean_passes; ++pass) {
-        SP_ROW_LAUNCH(k_row_geo, Gm, wm, s->A.rp, s->A.v, m, r);
-        apply(r, ones_n);
-        SP_ROW_LAUNCH(k_row_geo, Gn, wn, s->AT.rp, s->AT.v, n, c);
-        apply(ones_m, c);
-    }
-    for (uint64_t it = 0; it < P.ruiz_iterations; ++it) {
-        SP_ROW_LAUNCH(k_row_ruiz, Gm, wm, s->A.rp, s->A.v, m, r);
-        SP_ROW_LAUNCH(k_row_ruiz, Gn, wn, s->AT.rp, s->AT.v, n, c);
-        apply(r, c);
-    }
-    if (P.pock_chambolle_enabled) {
-        k_row_pc<<<gm, NT, 0, st>>>(s->A.rp, s->A.v, m, P.pock_chambolle_alpha, r);
-        k_row_pc<<<gn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, 2.0 - P.pock_chambolle_alpha, c);
-        apply(r, c);
-    }
-    // Original bounds and objective come in through the output slots of the scaled ones.
-    double *oc, *olc, *ouc, *olv, *ouv;
+    // The original bounds and objective come in through the output slots of the scaled
+    // ones. They are copied first: a copy from pageable memory waits for the work queued
+    // before it on the stream, and the sweeps below are meant to run while the host
+    // goes on (plan_transpose).
+    double *oc = nullptr, *olc = nullptr, *ouc = nullptr, *olv = nullptr, *ouv = nullptr;
     if ((rc = upload_vec(ctx, &oc, lp->c, n)) || (rc = upload_vec(ctx, &olc, lp->lc, m)) ||
         (rc = upload_vec(ctx, &ouc, lp->uc, m)) || (rc = upload_vec(ctx, &olv, lp->lv, n)) ||
-        (rc = upload_vec(ctx, &ouv, lp->uv, n)))
+        (rc = upload_vec(ctx, &ouv, lp->uv, n))) {
+        for (double *b : {oc, olc, ouc, olv, ouv}) dfree(b, st);
         return rc;
-    // norms of the original problem (solver.rs:317-318)
+    }
+    auto release = [&]() {
+        for (double *b : {rb[0], rb[1], cb[0], cb[1]}) dfree(b, st);
+    };
+    if ((rc = dalloc(&rb[0], m)) || (rc = dalloc(&rb[1], m)) || (rc = dalloc(&cb[0], n)) || (rc = dalloc(&cb[1], n))) {
+        release();
+        for (double *b : {oc, olc, ouc, olv, ouv}) dfree(b, st);
+        return rc;
+    }
+    const int gm = grid_of(ctx, m), gn = grid_of(ctx, n);
+    // lanes per row of the row sweeps: the smallest power of two g >= 2 with 2.5·g at
+    // least the median row length (of 4096 rows spread over the layout), at most 32; the
+    // rows longer than SWEEP_TRIPS·g go to whole warps (on the 40M LP: g = 8 for A', whose
+    // rows hold 20 entries on average, and 2 for A'ᵀ, whose median row holds 3)
+    auto group_of = [](auto row_len, int64_t rows) {
+        if (rows <= 0) return 2;
+        const int64_t samples = std::min<int64_t>(rows, 4096);
+        std::vector<int64_t> len(samples);
+        for (int64_t q = 0; q < samples; ++q) len[q] = row_len(q * rows / samples);
+        std::nth_element(len.begin(), len.begin() + samples / 2, len.end());
+        const int64_t med = len[samples / 2];
+        int g = 2;
+        while (g < 32 && 5 * g < 2 * med) g *= 2;
+        return g;
+    };
+    const int64_t *arp = lp->a.row_ptr;
+    const int Gm = group_of([&](int64_t i) { return arp[i + 1] - arp[i]; }, m);
+    const int Gn = group_of([&](int64_t j) { return (int64_t)rp_t[j + 1] - rp_t[j]; }, n);
+    const int wm = grid_of(ctx, m * Gm), wn = grid_of(ctx, n * Gn);
+    k_fill<<<gm, NT, 0, st>>>(s->row_scale, 1.0, m);
+    k_fill<<<gn, NT, 0, st>>>(s->col_scale, 1.0, n);
+    // sweep over A' (rows i) or A'ᵀ (rows j): own = the layout's row factors, gat = the others
+    auto sweep = [&](bool a_side, bool geo2, int next, const double *own, const double *gat, double *nxt) {
+        const DevCsr &M = a_side ? s->A : s->AT;
+        double *scale = a_side ? s->row_scale : s->col_scale;
+        with_group(a_side ? Gm : Gn, [&](auto G) {
+            launch_sweep<decltype(G)::value>(M, geo2, next, a_side ? wm : wn, st, own, gat, scale, nxt);
+        });
+    };
+    const uint64_t GP = P.geometric_mean_passes, RZ = P.ruiz_iterations;
+    if (nnz > 0) {  // with no entries every factor is 1 (inv_sqrt of 0) and the scales stay 1
+        int ri = 0, cc = 0;  // which of rb / cb holds the current factors
+        if (GP > 0) {
+            // geometric-mean passes (scaling.rs:60-66): the first row factors from A' as
+            // given, each later one from the sweep that finished the pass before
+            with_group(Gm, [&](auto G) {
+                k_row_geo<decltype(G)::value><<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, rb[0]);
+            });
+            for (uint64_t p = 0; p < GP; ++p) {
+                const bool last = p + 1 == GP;
+                const int next_t = last && RZ > 0 ? NEXT_MAX : NEXT_NONE;
+                with_group(Gn, [&](auto G) {
+                    constexpr int g = decltype(G)::value;
+                    if (next_t == NEXT_MAX)
+                        k_scale_geo_cols<g, NEXT_MAX><<<wn, NT, 0, st>>>(s->AT.rp, s->AT.ci, s->AT.v, n, rb[ri], cb[0],
+                                                                         s->col_scale, cb[1]);
+                    else
+                        k_scale_geo_cols<g, NEXT_NONE><<<wn, NT, 0, st>>>(s->AT.rp, s->AT.ci, s->AT.v, n, rb[ri], cb[0],
+                                                                          s->col_scale, nullptr);
+                });
+                sweep(true, true, !last ? NEXT_GEO : (RZ > 0 ? NEXT_MAX : NEXT_NONE), rb[ri], cb[0], rb[ri ^ 1]);
+                ri ^= 1;
+            }
+            cc = 1;  // the first Ruiz column factors (written by the last pass's A'ᵀ sweep)
+        } else if (RZ > 0) {
+            with_group(Gm, [&](auto G) {
+                k_row_ruiz<decltype(G)::value><<<wm, NT, 0, st>>>(s->A.rp, s->A.v, m, rb[0]);
+            });
+            with_group(Gn, [&](auto G) {
+                k_row_ruiz<decltype(G)::value><<<wn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, cb[0]);
+            });
+        }
+        // Ruiz iterations (scaling.rs:67-72): both factors from the same matrix, so each
+        // sweep reads the current pair and writes the next into the other buffer
+        for (uint64_t q = 0; q < RZ; ++q) {
+            const int next = q + 1 < RZ ? NEXT_MAX : NEXT_NONE;
+            sweep(true, false, next, rb[ri], cb[cc], rb[ri ^ 1]);
+            sweep(false, false, next, cb[cc], rb[ri], cb[cc ^ 1]);
+            ri ^= 1;
+            cc ^= 1;
+        }
+        if (P.pock_chambolle_enabled) {  // scaling.rs:73-79: sums in index order, one row per thread
+            k_row_pc<<<gm, NT, 0, st>>>(s->A.rp, s->A.v, m, P.pock_chambolle_alpha, rb[0]);
+            k_row_pc<<<gn, NT, 0, st>>>(s->AT.rp, s->AT.v, n, 2.0 - P.pock_chambolle_alpha, cb[0]);
+            sweep(true, false, NEXT_NONE, rb[0], cb[0], nullptr);
+            sweep(false, false, NEXT_NONE, cb[0], rb[0], nullptr);
+        }
+    }
+    release();
     k_scale_vectors<<<std::max(gm, gn), NT, 0, st>>>(oc, olc, ouc, olv, ouv, s->row_scale, s->col_scale, s->c, s->lc,
                                                      s->uc, s->lv, s->uv, m, n);
-    k_seq_norms<<<4, NT, 0, st>>>(olc, ouc, oc, s->lc, s->uc, s->c, m, n, s->norms);
-    k_rescale<<<std::max(gm, gn), NT, 0, st>>>(s->lc, s->uc, s->lv, s->uv, s->c, s->norms, m, n,
-                                               P.bound_objective_rescaling, s->scales);
-    k_factors<<<std::max(gm, gn), NT, 0, st>>>(s->row_scale, s->col_scale, s->scales, s->pf, s->df, m, n);
+    dfree(olv, st);
+    dfree(ouv, st);
     SP_CUDA_TRY(cudaGetLastError());
-    SP_CUDA_TRY(cudaStreamSynchronize(st));
-    for (double *b : {r, c, ones_m, ones_n, oc, olc, ouc, olv, ouv}) dfree(b, st);
+    // the norms (of the original problem too, solver.rs:317-318), the rescaling and the
+    // residual factors, on the second stream
+    SP_CUDA_TRY(cudaEventRecord(ctx->aux_ev, st));
+    SP_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->aux_ev, 0));
+    side->arm(s, oc, olc, ouc);
+    cudaStream_t ax = ctx->aux;
+    // Each norm's block asks for all the shared memory a CTA may have, so that no other
+    // CTA shares its SM: beside the power iteration's CTAs the chain of additions ran 2-3
+    // times slower (4M terms: 22 ms alone, 45-60 ms beside a gather-bound kernel).
+    int optin = 0;
+    SP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    cudaFuncAttributes fa{};
+    SP_CUDA_TRY(cudaFuncGetAttributes(&fa, (const void *)k_seq_norms));
+    const int pad = std::max(0, optin - (int)fa.sharedSizeBytes);
+    SP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_seq_norms, cudaFuncAttributeMaxDynamicSharedMemorySize, pad));
+    k_seq_norms<<<4, NT, pad, ax>>>(olc, ouc, oc, s->lc, s->uc, s->c, m, n, s->norms);
+    k_rescale<<<std::max(gm, gn), NT, 0, ax>>>(s->lc, s->uc, s->lv, s->uv, s->c, s->norms, m, n,
+                                               P.bound_objective_rescaling, s->scales);
+    k_factors<<<std::max(gm, gn), NT, 0, ax>>>(s->row_scale, s->col_scale, s->scales, s->pf, s->df, m, n);
+    SP_CUDA_TRY(cudaGetLastError());
     return SP_OK;
-#undef SP_ROW_LAUNCH
 }
 
 // A'ᵀ on the device: a stable radix sort of the column indices (cub) gives, per
 // column, its entries in increasing row order: CsrMatrix::transpose's order
 // (problem.rs:88-109), bit for bit.
-int transpose_on_device(sp_solver *s) {
+int transpose_on_device(sp_solver *s, std::vector<int> &rp32) {
     sp_ctx *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
     const int64_t m = s->m, n = s->n, nnz = s->nnz;
@@ -1155,23 +1449,36 @@ int transpose_on_device(sp_solver *s) {
     SP_CUDA_TRY(cudaGetLastError());
     SP_CUDA_TRY(cudaStreamSynchronize(st));
     for (void *b : {(void *)row_of, (void *)keys_out, (void *)perm_in, (void *)perm_out, tmp}) dfree(b, st);
-    // tile plan of A'ᵀ from its row pointers
-    std::vector<int> rp32(n + 1);
+    // the row pointers for the host's tile plan (plan_transpose), which the scaling
+    // sweeps do not need: the host builds it while they run
+    rp32.resize(n + 1);
     SP_CUDA_TRY(cudaMemcpyAsync(rp32.data(), T.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
     SP_CUDA_TRY(cudaStreamSynchronize(st));
+    return SP_OK;
+}
+
+// The tile plan and row schedule of A'ᵀ, from its row pointers, built on the host and
+// uploaded (the SpMV engines and the power iteration need them). Both are built before
+// the first copy: a copy from pageable memory waits for the work queued before it on
+// the stream (the scaling sweeps), and the host work is meant to run beside that.
+int plan_transpose(sp_solver *s, const std::vector<int> &rp32) {
+    cudaStream_t st = s->ctx->stream;
+    const int64_t n = s->n;
+    DevCsr &T = s->AT;
     std::vector<int64_t> rp64(rp32.begin(), rp32.end());
     std::vector<Tile> tiles = build_tiles(rp64.data(), n);
     T.ntiles = (int)tiles.size();
     T.nlong = count_long_tiles(tiles);
+    const std::vector<uint16_t> sched = build_schedule(rp64.data(), n, tiles);
+    int rc;
     // Memory from the stream-ordered pool is ours only in the order of `st` (the pool may hand
     // out memory whose previous owner, on another stream, is still running, with a wait
     // for it inserted into `st`): every copy into it goes through `st`, never through the
     // legacy stream of a synchronous cudaMemcpy.
     if ((rc = dmalloc((void **)&T.tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1)))) return rc;
+    if ((rc = dalloc(&T.sched, n))) return rc;
     if (!tiles.empty())
         SP_CUDA_TRY(cudaMemcpyAsync(T.tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, st));
-    const std::vector<uint16_t> sched = build_schedule(rp64.data(), n, tiles);
-    if ((rc = dalloc(&T.sched, n))) return rc;
     if (n) SP_CUDA_TRY(cudaMemcpyAsync(T.sched, sched.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice, st));
     SP_CUDA_TRY(cudaStreamSynchronize(st));  // the host vectors end here
     return SP_OK;
@@ -1216,7 +1523,8 @@ int power_iteration(sp_solver *s) {  // Solver::estimate_norm (solver.rs:215-242
         s->norm_est = 1.0;
         return SP_OK;
     }
-    k_power_init<<<1, NT, 0, st>>>(s->pv, s->n, s->ppart);
+    k_power_fill<<<grid_of(s->ctx, s->n), NT, 0, st>>>(s->pv, s->n);
+    k_power_init<<<1, NT, 0, st>>>(s->n, s->ppart);
     k_power_start<<<1, 32, 0, st>>>(s->ppart, s->d_st);
     const uint64_t maxit = s->prm.power_iterations;
     PowerA a{s->A.rp, s->A.ci, s->A.v, s->A.tiles, s->pv, s->ptmp, s->d_st, 0.0};
@@ -1360,29 +1668,29 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     const int64_t m = s->m, n = s->n;
     const int64_t nP = 0;
     (void)nP;
+    // the set-up work on the second stream (scale_on_device); an early return joins it
+    // before the solver's buffers are released
+    SideNorms side;
     auto cleanup = [&](int code) {
+        side.join();
         solver_release(s);
         return code;
     };
     if ((rc = upload_csr(ctx, &lp->a, &s->A, false))) return cleanup(rc);
     stage("upload");
-    if ((rc = transpose_on_device(s))) return cleanup(rc);
+    std::vector<int> rp_t;
+    if ((rc = transpose_on_device(s, rp_t))) return cleanup(rc);
     stage("transpose");
     if ((rc = dalloc(&s->c, n)) || (rc = dalloc(&s->lc, m)) || (rc = dalloc(&s->uc, m)) || (rc = dalloc(&s->lv, n)) ||
         (rc = dalloc(&s->uv, n)) || (rc = dalloc(&s->pf, m)) || (rc = dalloc(&s->df, n)) ||
         (rc = dalloc(&s->row_scale, m)) || (rc = dalloc(&s->col_scale, n)) || (rc = dalloc(&s->scales, 2)) ||
         (rc = dalloc(&s->norms, 4)))
         return cleanup(rc);
-    if ((rc = scale_on_device(s, lp))) return cleanup(rc);
+    if ((rc = scale_on_device(s, lp, rp_t, &side))) return cleanup(rc);
+    // the host's tile plan of A'ᵀ while the GPU runs the scaling sweeps
+    if ((rc = plan_transpose(s, rp_t))) return cleanup(rc);
+    rp_t = std::vector<int>();
     stage("scaling");
-    double hn[4], hs[2];
-    SP_CUDA_TRY(cudaMemcpyAsync(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost, ctx->stream));
-    SP_CUDA_TRY(cudaMemcpyAsync(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
-    SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    s->b_norm = hn[2];
-    s->c_norm = hn[3];
-    s->bound_scale = hs[0];
-    s->obj_scale = hs[1];
     if (s->mixed) {
         if ((rc = dalloc(&s->A.v32, s->nnz)) || (rc = dalloc(&s->AT.v32, s->nnz))) return cleanup(rc);
         k_to_f32<<<grid_of(ctx, s->nnz), NT, 0, ctx->stream>>>(s->A.v, s->A.v32, s->nnz);
@@ -1406,11 +1714,20 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     if ((rc = set_smem_limits())) return cleanup(rc);
     if ((rc = choose_engines(s))) return cleanup(rc);
     stage("engines");
-    // ‖A'‖₂ and η (solver.rs:316)
-    if ((rc = sp_solver_reset(s))) return cleanup(rc);
-    stage("buffers");
+    // ‖A'‖₂ and η (solver.rs:316), while the second stream forms the norms
     if ((rc = power_iteration(s))) return cleanup(rc);
     stage("power");
+    if (side.join() != cudaSuccess) return cleanup(fail(SP_ERR_CUDA, "set-up: norms on the second stream failed"));
+    double hn[4], hs[2];
+    SP_CUDA_TRY(cudaMemcpyAsync(hn, s->norms, sizeof hn, cudaMemcpyDeviceToHost, ctx->stream));
+    SP_CUDA_TRY(cudaMemcpyAsync(hs, s->scales, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+    SP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    s->b_norm = hn[2];
+    s->c_norm = hn[3];
+    s->bound_scale = hs[0];
+    s->obj_scale = hs[1];
+    if ((rc = sp_solver_reset(s))) return cleanup(rc);
+    stage("norms");
     DevParams dp{};
     const sp_solver_params &P = s->prm;
     dp.tolerance = P.tolerance;
