@@ -367,6 +367,10 @@ struct PowerA {  // tmp = A' (v * s)
     __device__ __forceinline__ void prod(int c, double val, double (&p)[1]) const {
         p[0] = val * (__ldg(v + c) * scale);  // the gather sees v after `scale(v, s)`
     }
+    // the SELL path's view (sell.cuh): the gathered vector and the same product
+    using GT = double;
+    __device__ __forceinline__ const double *gvec() const { return v; }
+    __device__ __forceinline__ double mul(double val, double g) const { return val * (g * scale); }
     __device__ __forceinline__ void row(int r, const double (&s)[1], double *, const Pre &) const { tmp[r] = s[0]; }
     __device__ void store(int, const double *) const {}
 };
