@@ -12,6 +12,10 @@ form, device-resident (inputs in HBM before the timed region); the mixed FP32-Sp
 state form is reported beside it. `e2e` times the public one-call API (sp_solve) from
 pinned host arrays to the solution back on the host, for K·64 iterations. The matrices
 (≥ 1.2 GB) are far larger than the 126 MB L2, so no flush is needed between steps.
+On one GPU the line also carries, under `forms`, both forms solved to 1e-6 end to end
+(checked by the independent checker), the batched form on the 4096-LP batch and a compact
+serving run (48 requests of up to 1e6 nonzeros); `--no-tolerance`, `--no-batch` and
+`--no-serve` leave them out.
 
 Other workloads (one JSON line each): transport (2000 x 2000 transportation LP),
 batch (the 4096-LP uneven batch, solves/s), serve (Poisson arrivals, p50/p99 latency).
@@ -52,6 +56,7 @@ def parse():
     ap.add_argument("--tolerance-limit-s", type=float, default=300.0, help="time limit of each to-tolerance solve")
     ap.add_argument("--no-tolerance", action="store_true", help="skip the solves to the tolerance")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form section of the default line")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving section of the default line")
     return ap.parse_args()
 
 
@@ -436,9 +441,11 @@ def run_ours(args):
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(lp, f64["scaled"], f64["norm_estimate"])
 
-    batch = None
+    batch = serve = None
     if args.workload == "powerlaw" and args.scale == 1.0 and not args.no_batch and dist.world == 1:
         batch = batch_compact(sp, backend, dist, args.seed)
+    if args.workload == "powerlaw" and args.scale == 1.0 and not args.no_serve and dist.world == 1:
+        serve = serve_compact(sp, backend, device, args.seed)
 
     clocks = f64["clocks"]
     line = {
@@ -478,6 +485,7 @@ def run_ours(args):
                       "note": "iter_per_s runs with tolerances of 0 (every epoch in FP32 SpMV); to_tolerance "
                               "is the solve to 1e-6, which moves the SpMV to FP64 below 1e-5"},
             "batch": batch,
+            "serve": serve,
         },
         "setup_s": f64["setup_s"],
     }
@@ -664,9 +672,9 @@ def run_batch(args):
     dist.close()
 
 
-def serve_requests(seed: int, count: int):
+def serve_requests(seed: int, count: int, max_nnz: float = 1e7):
     """(LP seed, m, n) of each request of the serving workload: nnz log-uniform in
-    [1e3, 1e7], n = nnz/5 columns of 5 entries, m = n/2 rows."""
+    [1e3, max_nnz], n = nnz/5 columns of 5 entries, m = n/2 rows."""
     import math
 
     import numpy as np
@@ -674,33 +682,31 @@ def serve_requests(seed: int, count: int):
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
-        nnz = math.exp(rng.uniform(math.log(1e3), math.log(1e7)))
+        nnz = math.exp(rng.uniform(math.log(1e3), math.log(max_nnz)))
         n = max(10, int(nnz / 5))
         out.append((seed * 7919 + i, max(5, n // 2), n))
     return out
 
 
-def run_serve(args):
-    """The serving loop under Poisson arrivals (λ = 200/s) of random LPs with nnz
-    log-uniform in [1e3, 1e7] (n = nnz/5, m = n/2), tolerance 1e-6: p50/p99 time to
-    solution and solves/s, FP64 and mixed."""
+SERVE_MAX_ITERATIONS = 200_000
+
+
+def serve_forms(sp, backend, device, seed, nreq, max_nnz):
+    """The serving loop under Poisson arrivals (200/s) of `nreq` random LPs, tolerance 1e-6,
+    in both precisions: Optimal solves/s, p50/p99 time to solution over the requests that
+    reached Optimal, and every other request with its path and error, solved again alone
+    (untimed) for comparison."""
     import threading
 
     import numpy as np
 
-    import saddlepoint_b200 as sp
-
-    dist = Dist(args.gpus)
-    nreq = max(8, min(args.steps, 400))
-    specs = serve_requests(args.seed, nreq)
-    lps = [sp.generate_random_lp(seed, m, n, (5, 5)) for seed, m, n in specs]
-    gaps = np.random.default_rng(args.seed + 1).exponential(1.0 / 200.0, size=nreq)
-    backend = sp.CudaBackend(dist.local)
+    specs = serve_requests(seed, nreq, max_nnz)
+    lps = [sp.generate_random_lp(s, m, n, (5, 5)) for s, m, n in specs]
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / 200.0, size=nreq)
     forms = {}
     for prec in (sp.Precision.FP64, sp.Precision.Mixed):
-        srv = sp.Server(budget_bytes=150e9, max_inflight=8, batch_max_nnz=50_000,
-                        params=sp.SolverParams(tolerance=1e-6, max_iterations=200_000, precision=prec),
-                        backend=backend)
+        params = sp.SolverParams(tolerance=1e-6, max_iterations=SERVE_MAX_ITERATIONS, precision=prec)
+        srv = sp.Server(budget_bytes=150e9, max_inflight=8, batch_max_nnz=50_000, params=params, backend=backend)
         results = []
 
         def collect():
@@ -712,7 +718,7 @@ def run_serve(args):
         th = threading.Thread(target=collect)
         th.start()
         t0 = time.time()
-        with Clocks(dist.local) as clk:
+        with Clocks(device) as clk:
             due = t0
             index = {}
             for i, (lp, g) in enumerate(zip(lps, gaps)):
@@ -725,7 +731,6 @@ def run_serve(args):
         wall = time.time() - t0
         srv.close()
         # results that are neither Optimal nor the iteration cap, solved again alone (untimed)
-        params = sp.SolverParams(tolerance=1e-6, max_iterations=200_000, precision=prec)
         alone = {}
         for r in results:
             if r.status not in (0, 3):
@@ -737,7 +742,8 @@ def run_serve(args):
         ok = [r for r in results if r.status == 0]
         lat = np.array([r.total_s for r in ok]) if ok else np.array([float("nan")])
         lat_all = np.array([r.total_s for r in results])
-        forms[prec] = {"solves_per_s": len(ok) / wall, "requests_per_s": nreq / wall,
+        name = "fp64" if prec == sp.Precision.FP64 else "mixed"
+        forms[name] = {"solves_per_s": len(ok) / wall, "requests_per_s": nreq / wall,
                        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                        "latency_over": "requests that reached Optimal (time to 1e-6)",
                        "optimal": len(ok), "not_optimal": nreq - len(ok), "requests": nreq,
@@ -749,17 +755,40 @@ def run_serve(args):
                              "alone": alone.get(r.id)}
                             for r in results if r.status != 0), key=lambda d: d["index"]),
                        "p50_all_s": float(np.percentile(lat_all, 50)),
-                       "queue_p50_s": float(np.median([r.queue_s for r in results])), "clocks": clk.summary()}
-    f64 = forms[sp.Precision.FP64]
+                       "queue_p50_s": float(np.median([r.queue_s for r in results])), "wall_s": wall,
+                       "clocks": clk.summary()}
+    return forms
+
+
+def serve_compact(sp, backend, device, seed):
+    """The serving section of the default line: 48 requests of up to 1e6 nonzeros (the full
+    workload, `--workload serve`, goes to 1e7 and takes minutes per form)."""
+    forms = serve_forms(sp, backend, device, seed, 48, 1e6)
+    return {"workload": "Poisson arrivals 200/s, 48 requests, nnz log-uniform [1e3,1e6], n=nnz/5, m=n/2, tol 1e-6",
+            "budget_bytes": 150e9, "max_inflight": 8, "batch_max_nnz": 50_000,
+            "max_iterations": SERVE_MAX_ITERATIONS, **forms}
+
+
+def run_serve(args):
+    """The serving loop under Poisson arrivals (λ = 200/s) of random LPs with nnz
+    log-uniform in [1e3, 1e7] (n = nnz/5, m = n/2), tolerance 1e-6: p50/p99 time to
+    solution and solves/s, FP64 and mixed."""
+    import saddlepoint_b200 as sp
+
+    dist = Dist(args.gpus)
+    nreq = max(8, min(args.steps, 400))
+    backend = sp.CudaBackend(dist.local)
+    forms = serve_forms(sp, backend, dist.local, args.seed, nreq, 1e7)
+    f64 = forms["fp64"]
     line = {
         "metric": "serving solves/s and p50/p99 time to 1e-6 (Poisson 200/s)", "value": f64["solves_per_s"],
         "unit": "solves/s", "n_gpus": dist.world, "steps": nreq, "warmup": 0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
         "config": {"workload": "Poisson arrivals 200/s, nnz log-uniform [1e3,1e7], n=nnz/5, m=n/2",
                    "budget_bytes": 150e9, "max_inflight": 8, "batch_max_nnz": 50_000, "requests": nreq,
-                   "max_iterations": 200_000},
+                   "max_iterations": SERVE_MAX_ITERATIONS},
         "parallelism": f"replicas x{dist.world}",
-        "forms": {"fp64": f64, "mixed": forms[sp.Precision.Mixed]},
+        "forms": {"fp64": f64, "mixed": forms["mixed"]},
         "p50_s": f64["p50_s"], "p99_s": f64["p99_s"],
         "clocks": {k: f64["clocks"][k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
