@@ -82,8 +82,7 @@ inline std::vector<uint16_t> build_schedule(const int64_t *rp, int64_t nrows, co
     std::vector<uint16_t> sched((size_t)std::max<int64_t>(nrows, 0), 0);
     // tiles own disjoint rows: blocks of tiles go to host threads
     auto run = [&](size_t t0, size_t t1) {
-        std::vector<int> shortr, heavy, order;
-        std::vector<char> used;
+        std::vector<int> shortr, heavy, bank, nxt;
         for (size_t ti = t0; ti < t1; ++ti) {
             const Tile &t = tiles[ti];
             const int64_t r0 = t.x, nr = (int64_t)t.y - t.x, k0 = t.z;
@@ -91,42 +90,57 @@ inline std::vector<uint16_t> build_schedule(const int64_t *rp, int64_t nrows, co
                 sched[r0] = SCHED_WARP;
                 continue;
             }
-            shortr.clear();
+            // the short rows by decreasing length, ties in row order (a counting sort), and
+            // the heavy rows in row order
+            int start[SEQ_MAX + 2] = {};
             heavy.clear();
-            for (int q = 0; q < nr; ++q) (rp[r0 + q + 1] - rp[r0 + q] > SEQ_MAX ? heavy : shortr).push_back(q);
-            std::stable_sort(shortr.begin(), shortr.end(), [&](int a, int b) {
-                return rp[r0 + a + 1] - rp[r0 + a] > rp[r0 + b + 1] - rp[r0 + b];
-            });
-            order.clear();
-            used.assign(shortr.size(), 0);
-            size_t next = 0;
-            while (order.size() < shortr.size()) {
-                // one half-warp: distinct start banks among the next 64 candidates, then
-                // whatever comes next
+            for (int q = 0; q < nr; ++q) {
+                const int64_t len = rp[r0 + q + 1] - rp[r0 + q];
+                if (len > SEQ_MAX) heavy.push_back(q);
+                else ++start[SEQ_MAX - len + 1];
+            }
+            for (int l = 1; l <= SEQ_MAX + 1; ++l) start[l] += start[l - 1];
+            const int ns = start[SEQ_MAX + 1];
+            shortr.resize(ns);
+            bank.resize(ns);
+            for (int q = 0; q < nr; ++q) {
+                const int64_t len = rp[r0 + q + 1] - rp[r0 + q];
+                if (len <= SEQ_MAX) shortr[start[SEQ_MAX - len]++] = q;
+            }
+            for (int c = 0; c < ns; ++c) bank[c] = (int)((rp[r0 + shortr[c]] - k0) & 15);
+            // Half-warps of 16 rows in distinct start banks: among the next 64 rows not yet
+            // dealt, in sorted order, each whose bank is still free joins; the half-warp is
+            // then topped up with the first rows not yet dealt. The rows not yet dealt are a
+            // list (nxt, from the head node ns), so each half-warp looks at 64 of them at most.
+            nxt.resize(ns + 1);
+            for (int c = 0; c < ns; ++c) nxt[c] = c + 1;
+            nxt[ns] = ns > 0 ? 0 : ns;
+            const int head = ns, end = ns;
+            int out = 0;
+            while (nxt[head] != end) {
                 unsigned mask = 0;
                 int placed = 0, seen = 0;
-                for (size_t c = next; c < shortr.size() && placed < 16 && seen < 64; ++c) {
-                    if (used[c]) continue;
+                for (int p = head, c = nxt[head]; c != end && placed < 16 && seen < 64;) {
                     ++seen;
-                    const int bank = (int)((rp[r0 + shortr[c]] - k0) & 15);
-                    if (!((mask >> bank) & 1u)) {
-                        mask |= 1u << bank;
-                        used[c] = 1;
-                        order.push_back(shortr[c]);
+                    if (!((mask >> bank[c]) & 1u)) {
+                        mask |= 1u << bank[c];
+                        sched[r0 + out++] = (uint16_t)shortr[c];
                         ++placed;
+                        nxt[p] = nxt[c];
+                        c = nxt[p];
+                    } else {
+                        p = c;
+                        c = nxt[c];
                     }
                 }
-                for (size_t c = next; c < shortr.size() && placed < 16; ++c)
-                    if (!used[c]) {
-                        used[c] = 1;
-                        order.push_back(shortr[c]);
-                        ++placed;
-                    }
-                while (next < shortr.size() && used[next]) ++next;
+                while (placed < 16 && nxt[head] != end) {
+                    const int c = nxt[head];
+                    sched[r0 + out++] = (uint16_t)shortr[c];
+                    ++placed;
+                    nxt[head] = nxt[c];
+                }
             }
-            for (size_t i = 0; i < order.size(); ++i) sched[r0 + i] = (uint16_t)order[i];
-            for (size_t i = 0; i < heavy.size(); ++i)
-                sched[r0 + order.size() + i] = (uint16_t)(heavy[i] | SCHED_WARP);
+            for (size_t i = 0; i < heavy.size(); ++i) sched[r0 + out + i] = (uint16_t)(heavy[i] | SCHED_WARP);
         }
     };
     const size_t nt = tiles.size();
