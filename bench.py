@@ -742,6 +742,14 @@ def serve_forms(sp, backend, device, seed, nreq, max_nnz):
         ok = [r for r in results if r.status == 0]
         lat = np.array([r.total_s for r in ok]) if ok else np.array([float("nan")])
         lat_all = np.array([r.total_s for r in results])
+        by_path = {}
+        for pname in ("slot", "batch"):
+            sel = [r for r in ok if r.path == pname]
+            if sel:
+                t = np.array([r.total_s for r in sel])
+                by_path[pname] = {"optimal": len(sel), "p50_s": float(np.percentile(t, 50)),
+                                  "p99_s": float(np.percentile(t, 99)),
+                                  "iterations_median": float(np.median([r.iterations for r in sel]))}
         name = "fp64" if prec == sp.Precision.FP64 else "mixed"
         forms[name] = {"solves_per_s": len(ok) / wall, "requests_per_s": nreq / wall,
                        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
@@ -756,6 +764,7 @@ def serve_forms(sp, backend, device, seed, nreq, max_nnz):
                             for r in results if r.status != 0), key=lambda d: d["index"]),
                        "p50_all_s": float(np.percentile(lat_all, 50)),
                        "queue_p50_s": float(np.median([r.queue_s for r in results])), "wall_s": wall,
+                       "optimal_by_path": by_path,
                        "clocks": clk.summary()}
     return forms
 
