@@ -42,6 +42,7 @@ if ROOT not in sys.path:
 CASES = {
     "powerlaw_m200000_n400000_nnz3000000_seed3": ("powerlaw", (3, 200_000, 400_000, 3_000_000), 1e-6, 640),
     "transport_300x300_seed5": ("transport", (5, 300, 300), 1e-6, 640),
+    "transport_2000x2000_seed1": ("transport", (1, 2000, 2000), 1e-6, 640),
     "powerlaw_m2000000_n4000000_nnz40000000_seed1": ("powerlaw", (1, 2_000_000, 4_000_000, 40_000_000), 1e-6, 6400),
 }
 

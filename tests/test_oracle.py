@@ -283,7 +283,7 @@ def test_scale_fixtures_match_their_generated_lps():
     sys.path.insert(0, GOLDEN)
     from make_scale_goldens import fingerprint
 
-    for name in ("powerlaw_m200000_n400000_nnz3000000_seed3", "transport_300x300_seed5"):
+    for name in ("powerlaw_m200000_n400000_nnz3000000_seed3", "transport_300x300_seed5", "transport_2000x2000_seed1"):
         with open(os.path.join(GOLDEN, f"{name}.json")) as f:
             g = json.load(f)
         gen = oracle.generate_powerlaw_lp if g["generator"] == "powerlaw" else oracle.generate_transport_lp
