@@ -370,6 +370,14 @@ void sp_lp_release(sp_lp *lp);
  * message in err (any of the two may be null). Row and column names are not kept. */
 int sp_read_mps(const char *text, size_t len, sp_lp *out, int64_t *err_line, char *err, size_t errlen);
 
+/* LpProblem::validate (crates/saddlepoint-core/src/problem.rs:166-194), host code (no
+ * device needed): SP_OK, or SP_ERR_PROBLEM with the reference's message for the first
+ * failure in its order — a variable's bounds (NaN, then lower above upper) over all
+ * columns, then a constraint's, then a NaN coefficient among c and then A's values
+ * (numbered after c) — written into `message` (`cap` bytes; may be null). Every solve
+ * runs this check first and fails with the same code and message. */
+int sp_problem_validate(const sp_lp *lp, char *message, size_t cap);
+
 /* CsrMatrix::from_triplets (crates/saddlepoint-core/src/problem.rs:33-77) on the GPU of
  * `ctx`, for loading large problems: ntrip (row, column, value) triplets in host memory to
  * a CSR matrix with library-owned host arrays (release with sp_csr_release). Entries are

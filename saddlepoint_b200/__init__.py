@@ -32,7 +32,7 @@ __all__ = [
     "BackendError", "SolveError", "Status", "Termination", "Precision", "LpProblem", "ScaledProblem",
     "SolverParams", "Solution", "CudaBackend", "Solver", "solve", "solve_stepwise", "BatchSolver", "Server",
     "generate_random_lp", "generate_powerlaw_lp", "generate_transport_lp", "library", "read_mps", "MpsError",
-    "csr_from_triplets", "presolve", "Presolved", "solve_presolved", "polish",
+    "csr_from_triplets", "presolve", "Presolved", "solve_presolved", "polish", "validate",
 ]
 
 
@@ -584,6 +584,17 @@ class MpsError(ValueError):
     def __init__(self, line: int, msg: str):
         super().__init__(f"line {line}: {msg}")
         self.line, self.msg = line, msg
+
+
+def validate(problem) -> None:
+    """LpProblem::validate (crates/saddlepoint-core/src/problem.rs:166-194) in host code:
+    raises SolveError (code SP_ERR_PROBLEM) with the reference's message for the first
+    failure in its order; every solve runs the same check first."""
+    view = _LpView(LpProblem.from_any(problem))
+    buf = C.create_string_buffer(256)
+    rc = L.load().sp_problem_validate(C.byref(view.s), buf, 256)
+    if rc != L.SP_OK:
+        raise SolveError(rc, buf.value.decode())
 
 
 def read_mps(source, name: str = "") -> LpProblem:

@@ -170,6 +170,7 @@ SIGNATURES = [
     ("sp_generate", cint, [C.POINTER(GenParams), C.POINTER(Lp)]),
     ("sp_lp_release", None, [C.POINTER(Lp)]),
     ("sp_read_mps", cint, [C.c_char_p, C.c_size_t, C.POINTER(Lp), C.POINTER(i64), C.c_char_p, C.c_size_t]),
+    ("sp_problem_validate", cint, [C.POINTER(Lp), C.c_char_p, C.c_size_t]),
     ("sp_csr_from_triplets", cint, [VP, i64, i64, i64, PI64, PI64, PD, C.POINTER(Csr)]),
     ("sp_csr_release", None, [C.POINTER(Csr)]),
     ("sp_polish", cint, [VP, C.POINTER(Lp), C.POINTER(Params), dbl, PD, PD, C.POINTER(u64)]),

@@ -13,6 +13,7 @@
 #include <functional>
 #include <map>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -620,9 +621,21 @@ void parallel_for(int64_t n, const std::function<void(int64_t, int64_t)> &f) {
 std::map<const void *, Owned *> g_owned;
 std::mutex g_owned_mu;
 
+namespace sp {  // backend.cu: the calling thread's context and its last error
+int enter(sp_ctx *ctx);
+int fail(int code, const std::string &msg);
+}  // namespace sp
+
 extern "C" int sp_solve_stepwise(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *params, double *x, double *y,
                                  sp_solution_info *info) {
     if (!ctx || !lp) return SP_ERR_INVALID;
+    // problem.validate()? before anything else (solver.rs:155)
+    char msg[256] = "";
+    const int v = sp_problem_validate(lp, msg, sizeof msg);
+    if (v != SP_OK) {
+        if (sp::enter(ctx) == SP_OK) sp::fail(v, msg);
+        return v;
+    }
     sp_solver_params p;
     sp_solver_params_default(&p);
     if (params) p = *params;

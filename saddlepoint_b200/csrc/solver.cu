@@ -1510,26 +1510,68 @@ std::pair<int64_t, int> first_bad(int64_t len, const F &bad) {
     return {-1, 0};
 }
 
-int validate_lp(const sp_lp *lp) {  // LpProblem::validate (problem.rs:166-194)
-    const int64_t m = lp->a.nrows, n = lp->a.ncols;
-    // columns first, then rows, then coefficients; within each, the first failing index
-    const int col = first_bad(n, [&](int64_t j) {
-        if (std::isnan(lp->lv[j]) || std::isnan(lp->uv[j])) return 1;
-        if (lp->lv[j] > lp->uv[j]) return 2;
-        return std::isnan(lp->c[j]) ? 3 : 0;
-    }).second;
-    if (col == 1) return fail(SP_ERR_PROBLEM, "variable bound is NaN");
-    if (col == 2) return fail(SP_ERR_PROBLEM, "variable has lower bound above upper bound");
-    if (col == 3) return fail(SP_ERR_PROBLEM, "coefficient is NaN");
-    const int row = first_bad(m, [&](int64_t i) {
-        if (std::isnan(lp->lc[i]) || std::isnan(lp->uc[i])) return 1;
-        return lp->lc[i] > lp->uc[i] ? 2 : 0;
-    }).second;
-    if (row == 1) return fail(SP_ERR_PROBLEM, "constraint bound is NaN");
-    if (row == 2) return fail(SP_ERR_PROBLEM, "constraint has lower bound above upper bound");
-    if (first_bad(lp->a.nnz, [&](int64_t k) { return std::isnan(lp->a.values[k]) ? 1 : 0; }).second)
-        return fail(SP_ERR_PROBLEM, "coefficient is NaN");
-    return SP_OK;
+// A double as Rust's `{}` prints it: the shortest digits that read back to the same value,
+// written out without an exponent ("2", "0.1", "1500", "-0", "inf", "NaN").
+std::string rust_display(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    if (v == 0.0) return std::signbit(v) ? "-0" : "0";
+    char buf[64];
+    for (int p = 0; p <= 17; ++p) {
+        snprintf(buf, sizeof buf, "%.*e", p, v);
+        if (strtod(buf, nullptr) == v) break;
+    }
+    // buf = [-]d[.ddd]e±XX
+    std::string m(buf), digits;
+    const bool neg = m[0] == '-';
+    const size_t e = m.find('e');
+    for (size_t k = neg ? 1 : 0; k < e; ++k)
+        if (m[k] != '.') digits += m[k];
+    const int exp10 = atoi(m.c_str() + e + 1);
+    std::string out = neg ? "-" : "";
+    if (exp10 >= 0) {
+        if ((int)digits.size() <= exp10 + 1) {
+            out += digits + std::string(exp10 + 1 - digits.size(), '0');
+        } else {
+            out += digits.substr(0, exp10 + 1) + "." + digits.substr(exp10 + 1);
+        }
+    } else {
+        out += "0." + std::string(-exp10 - 1, '0') + digits;
+    }
+    return out;
+}
+
+// LpProblem::validate (problem.rs:166-194), its checks in its order and its messages: the
+// variables' bounds (NaN, then crossed) over all columns, then the constraints', then NaN
+// among the coefficients c and then A's values (numbered after c). Empty when valid.
+std::string lp_problem_error(const sp_lp *lp) {
+    const int64_t m = lp->a.nrows, n = lp->a.ncols, nnz = lp->a.nnz;
+    auto bounds = [&](const char *what, const double *lo, const double *hi, int64_t len) -> std::string {
+        const auto f = first_bad(len, [&](int64_t i) {
+            if (std::isnan(lo[i]) || std::isnan(hi[i])) return 1;
+            return lo[i] > hi[i] ? 2 : 0;
+        });
+        const std::string at = std::string(what) + " " + std::to_string(f.first);
+        if (f.second == 1) return at + " is NaN";
+        if (f.second == 2)
+            return at + " has lower bound " + rust_display(lo[f.first]) + " above upper bound " +
+                   rust_display(hi[f.first]);
+        return "";
+    };
+    std::string e = bounds("variable", lp->lv, lp->uv, n);
+    if (e.empty()) e = bounds("constraint", lp->lc, lp->uc, m);
+    if (!e.empty()) return e;
+    int64_t k = first_bad(n, [&](int64_t j) { return std::isnan(lp->c[j]) ? 1 : 0; }).first;
+    if (k < 0 && nnz > 0 && lp->a.values) {
+        k = first_bad(nnz, [&](int64_t q) { return std::isnan(lp->a.values[q]) ? 1 : 0; }).first;
+        if (k >= 0) k += n;
+    }
+    return k >= 0 ? "coefficient " + std::to_string(k) + " is NaN" : "";
+}
+
+int validate_lp(const sp_lp *lp) {
+    const std::string e = lp_problem_error(lp);
+    return e.empty() ? SP_OK : fail(SP_ERR_PROBLEM, e);
 }
 
 int power_iteration(sp_solver *s) {  // Solver::estimate_norm (solver.rs:215-242)
@@ -2105,6 +2147,15 @@ extern "C" int sp_solve(sp_ctx *ctx, const sp_lp *lp, const sp_solver_params *pa
     sp_solver_free(s);
     mark("free");
     return rc;
+}
+
+extern "C" int sp_problem_validate(const sp_lp *lp, char *message, size_t cap) {
+    if (!lp || !lp->c || !lp->lc || !lp->uc || !lp->lv || !lp->uv || lp->a.nrows < 0 || lp->a.ncols < 0 ||
+        lp->a.nnz < 0)
+        return SP_ERR_INVALID;
+    const std::string e = sp::lp_problem_error(lp);
+    if (message && cap > 0) snprintf(message, cap, "%s", e.c_str());
+    return e.empty() ? SP_OK : SP_ERR_PROBLEM;
 }
 
 extern "C" int sp_solver_scaled(sp_solver *s, int64_t *a_row_ptr, int32_t *a_col_idx, double *a_values,

@@ -1,0 +1,102 @@
+"""LpProblem::validate (crates/saddlepoint-core/src/problem.rs:166-194) as the library runs it
+before every solve (host code, no GPU): the reference's checks in its order — every
+variable's bounds, then every constraint's, then NaN among c and A's values — and its
+messages, including over ranges that the library scans on several host threads."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import saddlepoint_b200 as sp
+
+NAN, INF = math.nan, math.inf
+
+
+def small():
+    lp = sp.generate_random_lp(3, 12, 24, (2, 4))
+    for k in ("c", "lc", "uc", "lv", "uv", "values"):
+        setattr(lp, k, np.array(getattr(lp, k), dtype=np.float64, copy=True))
+    return lp
+
+
+def message(lp):
+    with pytest.raises(sp.SolveError) as e:
+        sp.validate(lp)
+    assert e.value.code == 6  # SP_ERR_PROBLEM
+    return str(e.value).split(": ", 1)[1]
+
+
+def test_a_valid_problem_passes():
+    sp.validate(small())
+
+
+@pytest.mark.parametrize("edit,expected", [
+    (lambda p: p.lv.__setitem__(3, NAN), "variable 3 is NaN"),
+    (lambda p: p.uv.__setitem__(3, NAN), "variable 3 is NaN"),
+    (lambda p: (p.lv.__setitem__(5, 2.0), p.uv.__setitem__(5, 1.0)), "variable 5 has lower bound 2 above upper bound 1"),
+    (lambda p: (p.lc.__setitem__(2, 1.5), p.uc.__setitem__(2, -0.25)),
+     "constraint 2 has lower bound 1.5 above upper bound -0.25"),
+    (lambda p: p.lc.__setitem__(0, NAN), "constraint 0 is NaN"),
+    (lambda p: p.c.__setitem__(4, NAN), "coefficient 4 is NaN"),
+    (lambda p: p.values.__setitem__(7, NAN), "coefficient 31 is NaN"),  # numbered after the 24 costs
+    (lambda p: (p.lv.__setitem__(1, INF), p.uv.__setitem__(1, 5.0)), "variable 1 has lower bound inf above upper bound 5"),
+    (lambda p: (p.lv.__setitem__(1, 1e20), p.uv.__setitem__(1, 1e-7)),
+     "variable 1 has lower bound 100000000000000000000 above upper bound 0.0000001"),
+])
+def test_each_failure_has_the_reference_message(edit, expected):
+    lp = small()
+    edit(lp)
+    assert message(lp) == expected
+    assert not oracle.validate(lp)
+
+
+def test_the_reference_order_decides_between_failures():
+    lp = small()
+    lp.c[0] = NAN
+    lp.lc[9], lp.uc[9] = 1.0, 0.0
+    assert message(lp) == "constraint 9 has lower bound 1 above upper bound 0"  # bounds before coefficients
+    lp.lv[7] = NAN
+    assert message(lp) == "variable 7 is NaN"  # variables before constraints
+    lp.lv[3], lp.uv[3] = 4.0, 3.0
+    assert message(lp) == "variable 3 has lower bound 4 above upper bound 3"  # the first column with either
+
+
+def big(n):
+    """One row of two entries over n columns (n large enough that the scans are split)."""
+    rp = np.array([0, 2], dtype=np.int64)
+    ci = np.array([0, 1], dtype=np.int32)
+    return sp.LpProblem(1, n, rp, ci, np.array([1.0, 1.0]), np.zeros(n), np.array([-1.0]), np.array([1.0]),
+                        np.zeros(n), np.ones(n))
+
+
+def test_the_first_failure_wins_across_the_split_scans():
+    n = 2_000_000
+    lp = big(n)
+    sp.validate(lp)
+    lp.lv[1_900_000], lp.uv[1_900_000] = 3.0, 2.0
+    lp.uv[1_200_000] = NAN
+    lp.c[5] = NAN
+    assert message(lp) == "variable 1200000 is NaN"
+    lp.uv[1_200_000] = 1.0
+    assert message(lp) == "variable 1900000 has lower bound 3 above upper bound 2"
+    lp.lv[1_900_000] = 0.0
+    assert message(lp) == "coefficient 5 is NaN"
+    lp.c[5] = 0.0
+    lp.values[1] = NAN
+    assert message(lp) == f"coefficient {n + 1} is NaN"
+
+
+def test_agrees_with_the_oracle_on_random_faults():
+    rng = np.random.default_rng(9)
+    for _ in range(60):
+        lp = small()
+        for _ in range(int(rng.integers(0, 3))):
+            k = ("c", "lc", "uc", "lv", "uv", "values")[int(rng.integers(0, 6))]
+            v = getattr(lp, k)
+            v[int(rng.integers(0, len(v)))] = (NAN, -5.0, 5.0, INF, -INF)[int(rng.integers(0, 5))]
+        ok = oracle.validate(lp)
+        if ok:
+            sp.validate(lp)
+        else:
+            message(lp)
