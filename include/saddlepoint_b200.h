@@ -266,7 +266,8 @@ typedef struct {
                           device solver (sp_solve) */
 } sp_batch_result;
 
-/* Scales and uploads `count` LPs into one packed arena. */
+/* Scales and uploads `count` LPs into one packed arena. An invalid LP (sp_problem_validate)
+ * fails the call with SP_ERR_PROBLEM and "instance <i>: <message>". */
 int sp_batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_params *params, sp_batch **out);
 /* Solves every instance; results[count]. An instance still running in the
  * persistent kernel SP_BATCH_HANDOFF_S seconds (environment, default 2; 0 turns
@@ -302,7 +303,8 @@ typedef struct {
 } sp_server_result;
 
 int sp_server_create(sp_ctx *ctx, const sp_server_config *cfg, const sp_solver_params *params, sp_server **out);
-/* Copies the LP; returns at once with a request id. */
+/* Copies the LP; returns at once with a request id. An invalid LP (sp_problem_validate) is
+ * refused with SP_ERR_PROBLEM and the message in sp_ctx_last_error of the server's context. */
 int sp_server_submit(sp_server *s, const sp_lp *lp, int64_t *id);
 /* Waits for the next finished request (timeout_s < 0: wait forever). Returns
  * SP_OK with *got = 1 when a result was written, *got = 0 on timeout. x and y may

@@ -137,7 +137,7 @@ class Server:
         p = sp.LpProblem.from_any(problem)
         view = sp._LpView(p)
         rid = C.c_int64()
-        self.backend._check(self.lib.sp_server_submit(self.h, C.byref(view.s), C.byref(rid)))
+        self.backend._check(self.lib.sp_server_submit(self.h, C.byref(view.s), C.byref(rid)), sp.SolveError)
         self._shapes[rid.value] = (p.ncols, p.nrows)
         return rid.value
 

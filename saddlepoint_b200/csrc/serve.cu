@@ -234,6 +234,13 @@ extern "C" int sp_server_create(sp_ctx *ctx, const sp_server_config *cfg, const 
 
 extern "C" int sp_server_submit(sp_server *s, const sp_lp *lp, int64_t *id) {
     if (!s || !lp || !lp->a.row_ptr) return SP_ERR_INVALID;
+    // an invalid LP is turned away here, before it can share a batch with valid ones
+    char msg[256] = "";
+    const int v = sp_problem_validate(lp, msg, sizeof msg);
+    if (v != SP_OK) {
+        if (sp::enter(s->ctx) == SP_OK) sp::fail(v, msg);
+        return v;
+    }
     auto *r = new Request();
     const int64_t m = lp->a.nrows, n = lp->a.ncols, nnz = lp->a.nnz;
     r->rp.assign(lp->a.row_ptr, lp->a.row_ptr + m + 1);

@@ -226,3 +226,35 @@ def test_server_under_load_matches_solo_solves(gpu_backend):
         assert r.error == 0, r.message
         assert r.status == int(solo.status) and r.iterations == solo.iterations
         assert np.array_equal(r.x, solo.x) and np.array_equal(r.y, solo.y)
+
+
+def _with_nan_bound(lp):
+    bad = sp().LpProblem.from_any(lp)
+    bad.lv = np.array(bad.lv, dtype=np.float64, copy=True)
+    bad.lv[0] = math.nan
+    return bad
+
+
+def test_invalid_problems_are_refused_before_any_solve(batch_lps, gpu_backend):
+    """Every entry point validates as Solver::new does (solver.rs:155): sp_solve and the
+    stepwise solve fail with SP_ERR_PROBLEM and the reference's message, a batch names the
+    instance, and the server refuses the request at submit while it keeps serving others."""
+    bad = _with_nan_bound(batch_lps[1])
+    params = sp().SolverParams(tolerance=TOL)
+    for run in (sp().solve, sp().solve_stepwise):
+        with pytest.raises(sp().SolveError) as e:
+            run(bad, params, gpu_backend)
+        assert e.value.code == 6 and str(e.value).endswith("variable 0 is NaN")
+    with pytest.raises(sp().SolveError) as e:
+        sp().BatchSolver([batch_lps[0], bad], params, gpu_backend)
+    assert e.value.code == 6 and str(e.value).endswith("instance 1: variable 0 is NaN")
+    srv = sp().Server(budget_bytes=2e9, max_inflight=1, batch_max_nnz=0, params=params, backend=gpu_backend)
+    try:
+        with pytest.raises(sp().SolveError) as e:
+            srv.submit(bad)
+        assert e.value.code == 6
+        rid = srv.submit(batch_lps[0])
+        r = srv.poll(timeout=60.0)
+        assert r is not None and r.id == rid and r.error == 0 and r.status == 0
+    finally:
+        srv.close()
