@@ -1726,8 +1726,6 @@ extern "C" int sp_solver_create(sp_ctx *ctx, const sp_lp *lp, const sp_solver_pa
     s->maximize = lp->maximize;
     if (s->prm.check_every == 0) s->prm.check_every = 1ull << 62;  // never a multiple: only the iteration limit checks
     const int64_t m = s->m, n = s->n;
-    const int64_t nP = 0;
-    (void)nP;
     // the set-up work on the second stream (scale_on_device); an early return joins it
     // before the solver's buffers are released
     SideNorms side;
