@@ -100,3 +100,17 @@ def test_agrees_with_the_oracle_on_random_faults():
             sp.validate(lp)
         else:
             message(lp)
+
+
+def test_problems_without_rows_or_columns():
+    """Empty ranges validate (the reference's loops simply do not run); a NaN bound on the one
+    column of a row-less problem is still found."""
+    empty_rows = sp.LpProblem(0, 3, np.array([0], dtype=np.int64), np.zeros(0, dtype=np.int32), np.zeros(0),
+                              np.ones(3), np.zeros(0), np.zeros(0), np.zeros(3), np.ones(3))
+    sp.validate(empty_rows)
+    empty_cols = sp.LpProblem(2, 0, np.array([0, 0, 0], dtype=np.int64), np.zeros(0, dtype=np.int32), np.zeros(0),
+                              np.zeros(0), np.array([-1.0, -INF]), np.array([1.0, 0.0]), np.zeros(0), np.zeros(0))
+    sp.validate(empty_cols)
+    one = sp.LpProblem(0, 1, np.array([0], dtype=np.int64), np.zeros(0, dtype=np.int32), np.zeros(0),
+                       np.ones(1), np.zeros(0), np.zeros(0), np.array([NAN]), np.ones(1))
+    assert message(one) == "variable 0 is NaN"
