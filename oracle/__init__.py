@@ -194,6 +194,7 @@ def lib():
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         L.or_lp_validate.argtypes = [C.POINTER(Lp)]
+        L.or_lp_validate_at.argtypes = [C.POINTER(Lp), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]
         L.or_generate.argtypes = [C.POINTER(GenParams), C.POINTER(Lp)]
     return _lib
 
@@ -509,6 +510,27 @@ def check(p, x, y) -> KktReport:
 
 def validate(p) -> bool:
     return lib().or_lp_validate(C.byref(_LpView(p).s)) == 0
+
+
+def validate_message(p) -> str:
+    """LpProblem::validate's error text (problem.rs:148-154, 166-194) for the first failure, ""
+    when the problem is valid; numbers as Rust's `{}` prints an f64 (shortest round trip,
+    never an exponent)."""
+    import numpy as np
+
+    what, kind, index = C.c_int(), C.c_int(), C.c_int64()
+    if lib().or_lp_validate_at(C.byref(_LpView(p).s), C.byref(what), C.byref(kind), C.byref(index)) == 0:
+        return ""
+    name = ("variable", "constraint", "coefficient")[what.value]
+    i = index.value
+    if kind.value == 1:
+        return f"{name} {i} is NaN"
+    lo, hi = (p.lv, p.uv) if what.value == 0 else (p.lc, p.uc)
+
+    def num(v):
+        return np.format_float_positional(float(v), trim="-")
+
+    return f"{name} {i} has lower bound {num(lo[i])} above upper bound {num(hi[i])}"
 
 
 class CpuBackend:

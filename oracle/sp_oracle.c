@@ -272,20 +272,39 @@ void or_csr_scale(or_csr *a, const double *row, const double *col) {
 }
 
 /* LpProblem::validate (problem.rs:166-194). */
-int or_lp_validate(const or_lp *p) {
+/* LpProblem::validate (problem.rs:166-194) with the first failure it reports: *what 0 for a
+ * variable, 1 a constraint, 2 a coefficient; *kind 1 NaN (ProblemError::NaN), 2 crossed
+ * bounds (ProblemError::CrossedBounds); *index within that family, the coefficients
+ * numbered c first, then A's values (the reference chains c with a.values). */
+int or_lp_validate_at(const or_lp *p, int *what, int *kind, int64_t *index) {
     int64_t m = p->a.nrows, n = p->a.ncols;
     const double *lo[2] = {p->lv, p->lc}, *hi[2] = {p->uv, p->uc};
     int64_t len[2] = {n, m};
+    *what = *kind = 0;
+    *index = -1;
     for (int s = 0; s < 2; ++s)
         for (int64_t i = 0; i < len[s]; ++i) {
-            if (isnan(lo[s][i]) || isnan(hi[s][i])) return OR_ERR_PROBLEM;
-            if (lo[s][i] > hi[s][i]) return OR_ERR_PROBLEM;
+            if (isnan(lo[s][i]) || isnan(hi[s][i]) || lo[s][i] > hi[s][i]) {
+                *what = s;
+                *kind = (isnan(lo[s][i]) || isnan(hi[s][i])) ? 1 : 2;
+                *index = i;
+                return OR_ERR_PROBLEM;
+            }
         }
-    for (int64_t j = 0; j < n; ++j)
-        if (isnan(p->c[j])) return OR_ERR_PROBLEM;
-    for (int64_t k = 0; k < p->a.nnz; ++k)
-        if (isnan(p->a.values[k])) return OR_ERR_PROBLEM;
+    for (int64_t j = 0; j < n + p->a.nnz; ++j)
+        if (isnan(j < n ? p->c[j] : p->a.values[j - n])) {
+            *what = 2;
+            *kind = 1;
+            *index = j;
+            return OR_ERR_PROBLEM;
+        }
     return OR_OK;
+}
+
+int or_lp_validate(const or_lp *p) {
+    int what, kind;
+    int64_t index;
+    return or_lp_validate_at(p, &what, &kind, &index);
 }
 
 /* LpProblem::objective (problem.rs:198-201). */

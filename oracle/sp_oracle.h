@@ -129,6 +129,7 @@ int or_csr_copy(const or_csr *src, or_csr *dst);
 
 /* ---- LP ------------------------------------------------------------------- */
 int or_lp_validate(const or_lp *p);
+int or_lp_validate_at(const or_lp *p, int *what, int *kind, int64_t *index);
 double or_lp_objective(const or_lp *p, const double *x);
 void or_lp_free(or_lp *p);
 

@@ -48,7 +48,7 @@ def test_each_failure_has_the_reference_message(edit, expected):
     lp = small()
     edit(lp)
     assert message(lp) == expected
-    assert not oracle.validate(lp)
+    assert not oracle.validate(lp) and oracle.validate_message(lp) == expected
 
 
 def test_the_reference_order_decides_between_failures():
@@ -77,29 +77,32 @@ def test_the_first_failure_wins_across_the_split_scans():
     lp.lv[1_900_000], lp.uv[1_900_000] = 3.0, 2.0
     lp.uv[1_200_000] = NAN
     lp.c[5] = NAN
-    assert message(lp) == "variable 1200000 is NaN"
+    assert message(lp) == "variable 1200000 is NaN" == oracle.validate_message(lp)
     lp.uv[1_200_000] = 1.0
     assert message(lp) == "variable 1900000 has lower bound 3 above upper bound 2"
     lp.lv[1_900_000] = 0.0
     assert message(lp) == "coefficient 5 is NaN"
     lp.c[5] = 0.0
     lp.values[1] = NAN
-    assert message(lp) == f"coefficient {n + 1} is NaN"
+    assert message(lp) == f"coefficient {n + 1} is NaN" == oracle.validate_message(lp)
 
 
 def test_agrees_with_the_oracle_on_random_faults():
+    """The oracle restates the reference's checks and messages (oracle.validate_message):
+    the same verdict and the same text on LPs with up to two random faults."""
     rng = np.random.default_rng(9)
-    for _ in range(60):
+    for _ in range(200):
         lp = small()
-        for _ in range(int(rng.integers(0, 3))):
+        for _ in range(int(rng.integers(0, 4))):
             k = ("c", "lc", "uc", "lv", "uv", "values")[int(rng.integers(0, 6))]
             v = getattr(lp, k)
             v[int(rng.integers(0, len(v)))] = (NAN, -5.0, 5.0, INF, -INF)[int(rng.integers(0, 5))]
-        ok = oracle.validate(lp)
-        if ok:
+        expected = oracle.validate_message(lp)
+        if not expected:
+            assert oracle.validate(lp)
             sp.validate(lp)
         else:
-            message(lp)
+            assert message(lp) == expected
 
 
 def test_problems_without_rows_or_columns():
