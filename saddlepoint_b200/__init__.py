@@ -113,9 +113,19 @@ class LpProblem:
 
 
 class _LpView:
-    """Keeps the arrays of an LpProblem alive while C holds pointers to them."""
+    """Keeps the arrays of an LpProblem alive while C holds pointers to them. The C ABI takes
+    the lengths from nrows, ncols and the row pointers, so the arrays' own lengths are
+    checked here first, as LpProblem::validate checks them (problem.rs:168-177): SolveError
+    (SP_ERR_PROBLEM) "c has length 5, expected 24" and the like, before any pointer is handed
+    over."""
 
     def __init__(self, p: LpProblem):
+        m, n = int(p.nrows), int(p.ncols)
+        for what, v, want in (("c", p.c, n), ("lv", p.lv, n), ("uv", p.uv, n), ("lc", p.lc, m), ("uc", p.uc, m)):
+            if len(v) != want:
+                raise SolveError(L.SP_ERR_PROBLEM, f"{what} has length {len(v)}, expected {want}")
+        if len(p.row_ptr) != m + 1 or len(p.col_idx) != len(p.values):
+            raise SolveError(L.SP_ERR_PROBLEM, f"A has length {len(p.row_ptr)}, expected {m + 1}")
         self.rp = np.ascontiguousarray(p.row_ptr, dtype=np.int64)
         self.ci = np.ascontiguousarray(p.col_idx, dtype=np.int32)
         self.v = _f64(p.values)

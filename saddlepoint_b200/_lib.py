@@ -20,6 +20,7 @@ PI32 = C.POINTER(C.c_int32)
 VP = C.c_void_p
 
 SP_OK = 0
+SP_ERR_PROBLEM = 6
 SP_ERR_PARSE = 8
 ERRORS = {
     1: "CUDA error",

@@ -117,3 +117,21 @@ def test_problems_without_rows_or_columns():
     one = sp.LpProblem(0, 1, np.array([0], dtype=np.int64), np.zeros(0, dtype=np.int32), np.zeros(0),
                        np.ones(1), np.zeros(0), np.zeros(0), np.array([NAN]), np.ones(1))
     assert message(one) == "variable 0 is NaN"
+
+
+@pytest.mark.parametrize("field,length,expected", [
+    ("c", 5, "c has length 5, expected 24"),
+    ("lv", 30, "lv has length 30, expected 24"),
+    ("uc", 0, "uc has length 0, expected 12"),
+    ("row_ptr", 12, "A has length 12, expected 13"),
+])
+def test_array_lengths_are_checked_before_the_library_sees_them(field, length, expected):
+    """The C ABI takes lengths from nrows, ncols and the row pointers; the Python layer checks
+    the arrays' own lengths first, in the reference's order and words (problem.rs:168-177),
+    so a short array is an error and never an out-of-bounds read."""
+    lp = small()
+    v = getattr(lp, field)
+    setattr(lp, field, np.resize(v, length) if length else v[:0])
+    assert message(lp) == expected
+    with pytest.raises(sp.SolveError):
+        sp.presolve(lp)
