@@ -376,8 +376,11 @@ int sp_read_mps(const char *text, size_t len, sp_lp *out, int64_t *err_line, cha
  * device needed): SP_OK, or SP_ERR_PROBLEM with the reference's message for the first
  * failure in its order — a variable's bounds (NaN, then lower above upper) over all
  * columns, then a constraint's, then a NaN coefficient among c and then A's values
- * (numbered after c) — written into `message` (`cap` bytes; may be null). Every solve
- * runs this check first and fails with the same code and message. */
+ * (numbered after c) — written into `message` (`cap` bytes; may be null). Then the
+ * matrix's structure, which the reference's CsrMatrix keeps by construction: row pointers
+ * from 0 to nnz, never decreasing, column indices in [0, ncols) — SP_ERR_INVALID with a
+ * message naming the entry. Every solve, batch and server submission runs this check first
+ * and fails with the same code and message. */
 int sp_problem_validate(const sp_lp *lp, char *message, size_t cap);
 
 /* CsrMatrix::from_triplets (crates/saddlepoint-core/src/problem.rs:33-77) on the GPU of

@@ -356,8 +356,7 @@ int batch_create(sp_ctx *ctx, const sp_lp *lps, int count, const sp_solver_param
     for (int i = 0; i < count; ++i) {  // each instance as Solver::new validates it (solver.rs:155)
         char msg[256] = "";
         const int v = sp_problem_validate(&lps[i], msg, sizeof msg);
-        if (v == SP_ERR_PROBLEM) return fail(v, "instance " + std::to_string(i) + ": " + msg);
-        if (v != SP_OK) return fail(v, "sp_batch_create: instance " + std::to_string(i) + " lacks an array");
+        if (v != SP_OK) return fail(v, "instance " + std::to_string(i) + ": " + (msg[0] ? msg : "lacks an array"));
     }
     sp_solver_params P;
     sp_solver_params_default(&P);

@@ -1541,10 +1541,28 @@ std::string rust_display(double v) {
     return out;
 }
 
-// LpProblem::validate (problem.rs:166-194), its checks in its order and its messages: the
-// variables' bounds (NaN, then crossed) over all columns, then the constraints', then NaN
-// among the coefficients c and then A's values (numbered after c). Empty when valid.
-std::string lp_problem_error(const sp_lp *lp) {
+// Calls body(w, k0, k1) for up to 16 contiguous ranges [k0, k1) of [0, len), each on a host
+// thread of its own when there is more than one.
+template <class F>
+void split_ranges(int64_t len, const F &body) {
+    const int workers = (int)std::max<int64_t>(1, std::min<int64_t>(16, len >> 18));
+    if (workers == 1) {
+        body(0, 0, len);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int w = 0; w < workers; ++w) th.emplace_back(body, w, len * w / workers, len * (w + 1) / workers);
+    for (auto &t : th) t.join();
+}
+
+// LpProblem::validate (problem.rs:166-194), its checks in its order and with its messages
+// (SP_ERR_PROBLEM): the variables' bounds (NaN, then crossed) over all columns, then the
+// constraints', then NaN among the coefficients c and then A's values (numbered after c).
+// Then the matrix's structure, which a C caller can break although the reference's
+// CsrMatrix keeps it by construction (SP_ERR_INVALID): row pointers from 0 to nnz, never
+// decreasing, and column indices in [0, ncols) — an index out of range would make a pass
+// read outside its vector on the GPU. A's values and column indices are read in one pass.
+int lp_check(const sp_lp *lp, std::string *msg) {
     const int64_t m = lp->a.nrows, n = lp->a.ncols, nnz = lp->a.nnz;
     auto bounds = [&](const char *what, const double *lo, const double *hi, int64_t len) -> std::string {
         const auto f = first_bad(len, [&](int64_t i) {
@@ -1558,20 +1576,66 @@ std::string lp_problem_error(const sp_lp *lp) {
                    rust_display(hi[f.first]);
         return "";
     };
-    std::string e = bounds("variable", lp->lv, lp->uv, n);
-    if (e.empty()) e = bounds("constraint", lp->lc, lp->uc, m);
-    if (!e.empty()) return e;
-    int64_t k = first_bad(n, [&](int64_t j) { return std::isnan(lp->c[j]) ? 1 : 0; }).first;
-    if (k < 0 && nnz > 0 && lp->a.values) {
-        k = first_bad(nnz, [&](int64_t q) { return std::isnan(lp->a.values[q]) ? 1 : 0; }).first;
-        if (k >= 0) k += n;
+    *msg = bounds("variable", lp->lv, lp->uv, n);
+    if (msg->empty()) *msg = bounds("constraint", lp->lc, lp->uc, m);
+    if (!msg->empty()) return SP_ERR_PROBLEM;
+    const int64_t kc = first_bad(n, [&](int64_t j) { return std::isnan(lp->c[j]) ? 1 : 0; }).first;
+    if (kc >= 0) {
+        *msg = "coefficient " + std::to_string(kc) + " is NaN";
+        return SP_ERR_PROBLEM;
     }
-    return k >= 0 ? "coefficient " + std::to_string(k) + " is NaN" : "";
+    const int64_t *rp = lp->a.row_ptr;
+    const int32_t *ci = lp->a.col_idx;
+    const double *v = lp->a.values;
+    if (!rp || (nnz > 0 && (!ci || !v))) {
+        *msg = "A lacks an array";
+        return SP_ERR_INVALID;
+    }
+    // per range: the first NaN value, and the first column out of range before it
+    std::vector<std::pair<int64_t, int64_t>> found(16, {-1, -1});
+    split_ranges(nnz, [&](int w, int64_t k0, int64_t k1) {
+        int64_t fc = -1;
+        for (int64_t k = k0; k < k1; ++k) {
+            if (std::isnan(v[k])) {
+                found[w] = {k, fc};
+                return;
+            }
+            if (fc < 0 && (ci[k] < 0 || ci[k] >= n)) fc = k;
+        }
+        found[w] = {-1, fc};
+    });
+    int64_t nan_at = -1, col_at = -1;
+    for (const auto &f : found) {
+        if (nan_at < 0 && f.first >= 0) nan_at = f.first;
+        if (col_at < 0 && f.second >= 0) col_at = f.second;
+    }
+    if (nan_at >= 0) {
+        *msg = "coefficient " + std::to_string(n + nan_at) + " is NaN";
+        return SP_ERR_PROBLEM;
+    }
+    if (rp[0] != 0 || rp[m] != nnz) {
+        *msg = "A's row pointers run from " + std::to_string(rp[0]) + " to " + std::to_string(rp[m]) +
+               ", not from 0 to " + std::to_string(nnz);
+        return SP_ERR_INVALID;
+    }
+    const int64_t row = first_bad(m, [&](int64_t i) { return rp[i + 1] < rp[i] ? 1 : 0; }).first;
+    if (row >= 0) {
+        *msg = "A's row pointers decrease after row " + std::to_string(row);
+        return SP_ERR_INVALID;
+    }
+    if (col_at >= 0) {
+        *msg = "A's column index " + std::to_string(ci[col_at]) + " at entry " + std::to_string(col_at) +
+               " is out of range for " + std::to_string(n) + " columns";
+        return SP_ERR_INVALID;
+    }
+    msg->clear();
+    return SP_OK;
 }
 
 int validate_lp(const sp_lp *lp) {
-    const std::string e = lp_problem_error(lp);
-    return e.empty() ? SP_OK : fail(SP_ERR_PROBLEM, e);
+    std::string msg;
+    const int rc = lp_check(lp, &msg);
+    return rc ? fail(rc, msg) : SP_OK;
 }
 
 int power_iteration(sp_solver *s) {  // Solver::estimate_norm (solver.rs:215-242)
@@ -2151,9 +2215,10 @@ extern "C" int sp_problem_validate(const sp_lp *lp, char *message, size_t cap) {
     if (!lp || !lp->c || !lp->lc || !lp->uc || !lp->lv || !lp->uv || lp->a.nrows < 0 || lp->a.ncols < 0 ||
         lp->a.nnz < 0)
         return SP_ERR_INVALID;
-    const std::string e = sp::lp_problem_error(lp);
+    std::string e;
+    const int rc = sp::lp_check(lp, &e);
     if (message && cap > 0) snprintf(message, cap, "%s", e.c_str());
-    return e.empty() ? SP_OK : SP_ERR_PROBLEM;
+    return rc;
 }
 
 extern "C" int sp_solver_scaled(sp_solver *s, int64_t *a_row_ptr, int32_t *a_col_idx, double *a_values,

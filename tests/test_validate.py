@@ -135,3 +135,23 @@ def test_array_lengths_are_checked_before_the_library_sees_them(field, length, e
     assert message(lp) == expected
     with pytest.raises(sp.SolveError):
         sp.presolve(lp)
+
+
+def test_matrix_structure_is_checked_after_the_reference_checks():
+    """Row pointers from 0 to nnz and never decreasing, column indices in range: the C ABI
+    checks what the reference's CsrMatrix keeps by construction (SP_ERR_INVALID), so a bad
+    index is an error instead of a read outside a vector on the GPU."""
+    lp = small()
+    lp.col_idx = np.array(lp.col_idx, dtype=np.int32, copy=True)
+    lp.col_idx[5] = lp.ncols
+    with pytest.raises(sp.SolveError) as e:
+        sp.validate(lp)
+    assert e.value.code == 2 and str(e.value).endswith(f"A's column index {lp.ncols} at entry 5 is out of range for 24 columns")
+    lp.lv[0] = NAN  # the reference's checks come first
+    assert message(lp) == "variable 0 is NaN"
+    lp = small()
+    lp.row_ptr = np.array(lp.row_ptr, dtype=np.int64, copy=True)
+    lp.row_ptr[3], lp.row_ptr[4] = lp.row_ptr[4], lp.row_ptr[3]
+    with pytest.raises(sp.SolveError) as e:
+        sp.validate(lp)
+    assert e.value.code == 2 and "row pointers decrease after row" in str(e.value)
