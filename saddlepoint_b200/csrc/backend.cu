@@ -487,6 +487,14 @@ extern "C" int sp_problem_load(sp_ctx *ctx, const sp_csr *a, const sp_csr *at, c
         return fail(SP_ERR_INVALID, "sp_problem_load: null argument");
     if (at->nrows != a->ncols || at->ncols != a->nrows || at->nnz != a->nnz)
         return fail(SP_ERR_INVALID, "sp_problem_load: `at` is not the transpose's shape");
+    // a column index out of range would make the SpMV read outside its vector on the GPU
+    auto cols_ok = [](const sp_csr *M) {
+        if (M->nnz > 0 && !M->col_idx) return false;
+        for (int64_t k = 0; k < M->nnz; ++k)
+            if (M->col_idx[k] < 0 || M->col_idx[k] >= M->ncols) return false;
+        return true;
+    };
+    if (!cols_ok(a) || !cols_ok(at)) return fail(SP_ERR_INVALID, "sp_problem_load: a column index is out of range");
     auto *p = new sp_problem();
     p->ctx = ctx;
     p->m = a->nrows;
